@@ -1,0 +1,391 @@
+#!/usr/bin/env python
+"""Benchmark of the SuperCountingBloom build + stream-query path on B200.
+
+One step = the reference's `--stream-query-only` pipeline (src/main.rs:110-127, the command
+benchmark/common.py times) on the default-geometry short-read workload: clear the counter table,
+insert every read, freeze, then query every read's k-mers into the stream report.  The metric is
+indexed k-mers per second over the whole step (whole job, all ranks).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Arms:
+  ours       value   : inputs resident in HBM, device entry points, CUDA events on the stream
+             e2e     : scb_build_and_stream_query with pinned host inputs (H2D inside the step)
+             plain   : the one-launch-per-stage kernels, same measurement as value
+  reference  the reference's CPU pipeline (multi-threaded port with its structure: 1024 mutex
+             shards, bounded queue, all host threads) on a bounded sample of the same workload.
+
+N > 1 runs N independent replicas (one table and one read set per GPU); value = k-mers of all
+ranks / the slowest rank's time.  Rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+GEOM = dict(k=31, m=21, s=25, n_hashes=4, counter_bits=16, counter_slots_exponent=30, block_slots_exponent=9)
+METRIC = "k-mers/s (build + stream query)"
+WORKLOAD = ("default geometry, short reads: 100 Mbp uniform genome, 20x of 150 bp reads (13.3M reads, 2 Gbp), "
+            "both strands, 1% substitutions, 1% of bases N in runs of 1-10; k=31 m=21 s=25 h=4, 16-bit "
+            "counters, 2^30 slots (2 GiB), 2^9 slots per block")
+CPU_SAMPLE_READS = 200_000
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--scale", type=float, default=1.0, help="genome scale (same coverage) for quick runs")
+    p.add_argument("--no-plain", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    return p.parse_args()
+
+
+class Dist:
+    def __init__(self, gpus: int):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+
+            torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                    device_id=torch.device("cuda", self.local))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, v: float) -> float:
+        if not self.pg:
+            return v
+        import torch
+
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, v: float) -> float:
+        if not self.pg:
+            return v
+        import torch
+
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region (SM clock, throttle reasons)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+def measured_peaks() -> tuple[float, str]:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        return float(json.load(open(p))["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profile_traffic() -> dict | None:
+    """DRAM bytes per k-mer of the insert tile kernel from the committed ncu summary (a capture of
+    a smaller case, scaled per k-mer window to a full launch)."""
+    p = os.path.join(ROOT, "profiles", "insert_tile_traffic.json")
+    try:
+        return json.load(open(p))
+    except (OSError, ValueError):
+        return None
+
+
+def workload(rank: int, scale: float):
+    from scbf_b200 import workloads
+
+    return workloads.config2(seed=1 + rank, scale=scale)
+
+
+# ---------------------------------------------------------------------------------------
+def run_reference(args, dist: Dist):
+    if dist.rank != 0:
+        return
+    from oracle import oracle
+
+    data, offsets = workload(0, args.scale)
+    n = min(CPU_SAMPLE_READS, len(offsets) - 1)
+    so = offsets[: n + 1].copy()
+    sd = data[: int(so[-1])]
+    threads = os.cpu_count() or 1
+    cfg = oracle.make_config(GEOM["k"], GEOM["m"], GEOM["s"], GEOM["n_hashes"], GEOM["counter_bits"],
+                             GEOM["counter_slots_exponent"], GEOM["block_slots_exponent"], threads, 4096)
+    times, kmers = [], 0
+    for step in range(args.warmup + args.steps):
+        f = oracle.OracleFilter(cfg)
+        t0 = time.perf_counter()
+        r = f.port_build_and_stream_query(sd, so, threads=threads, queue=4096)
+        dt = time.perf_counter() - t0
+        f.close()
+        kmers = r["inserted_kmers"]
+        if step >= args.warmup:
+            times.append(dt)
+    total = sum(times)
+    value = kmers * len(times) / total
+    sample = f"first {n} reads ({kmers} k-mers) of the workload per step, fresh 2 GiB table each step"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "k-mers/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample": sample, "parallelism": f"{threads} host threads"},
+        "cpu_baseline": {"value": value, "unit": "k-mers/s", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "k-mers/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------------------
+def run_ours(args, dist: Dist):
+    import torch
+
+    from scbf_b200 import _lib
+    from scbf_b200 import api
+
+    torch.cuda.set_device(dist.local)
+    L = _lib.load()
+    data, offsets = workload(dist.rank, args.scale)
+    n_seqs = len(offsets) - 1
+    n_bytes = int(offsets[-1])
+    cfg = api.SuperCountingBloomConfig(k=GEOM["k"], m=GEOM["m"], s=GEOM["s"], n_hashes=GEOM["n_hashes"],
+                                       counter_bits=api.CounterBits(GEOM["counter_bits"]),
+                                       counter_slots_exponent=GEOM["counter_slots_exponent"],
+                                       block_slots_exponent=GEOM["block_slots_exponent"], threads=1, queue=4096)
+    ctx = api._create(cfg)
+    h = ctx.h
+    d_data = torch.from_numpy(data).to("cuda")
+    d_off = torch.from_numpy(offsets.view(np.int64)).to("cuda")
+    stream = torch.cuda.current_stream()
+    sp = C.c_void_p(stream.cuda_stream)
+
+    def check(st):
+        if st != 0:
+            raise RuntimeError(_lib.last_error())
+
+    km, sm = C.c_uint64(0), C.c_uint64(0)
+    rep = _lib.ScbReport()
+
+    def step():
+        check(L.scb_reset(h))
+        check(L.scb_insert_batch_device(h, d_data.data_ptr(), d_off.data_ptr(), n_seqs, n_bytes, sp, C.byref(km),
+                                        C.byref(sm)))
+        check(L.scb_freeze(h))
+        check(L.scb_query_report_device(h, d_data.data_ptr(), d_off.data_ptr(), n_seqs, n_bytes, sp,
+                                        C.byref(rep)))
+
+    def timed(steps: int) -> tuple[float, dict]:
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        check(L.scb_set_timing(h, 1))
+        dist.barrier()
+        torch.cuda.synchronize()
+        launches0 = L.scb_kernel_launches()
+        clocks = Clocks(dist.local)
+        clocks.start()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(steps):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        clk = clocks.stop()
+        dist.barrier()
+        ms = ev0.elapsed_time(ev1)
+        t = _lib.ScbTimings()
+        check(L.scb_get_timings(h, C.byref(t)))
+        check(L.scb_set_timing(h, 0))
+        return dist.max(ms), {"clocks": clk, "launches": L.scb_kernel_launches() - launches0,
+                               "pack_ms": t.pack_ms / steps, "insert_ms": t.insert_ms / steps,
+                               "query_ms": t.query_ms / steps}
+
+    # workload statistics for the algorithmic bytes (outside any timed region)
+    st = _lib.ScbStats()
+    check(L.scb_reset(h))
+    check(L.scb_batch_stats(h, data.ctypes.data, offsets.ctypes.data, n_seqs, C.byref(st)))
+
+    check(L.scb_set_strategy(h, 2, 2))
+    ms, info = timed(args.steps)
+    kmers = km.value
+    assert rep.valid_kmers == kmers, (rep.valid_kmers, kmers)
+    all_kmers = dist.sum(float(kmers))
+    value = all_kmers * args.steps / (ms / 1e3)
+    fused_report = (rep.valid_kmers, rep.positive_estimates, rep.estimate_checksum)
+
+    plain = None
+    if not args.no_plain:
+        check(L.scb_set_strategy(h, 1, 1))
+        p_steps = max(1, args.steps // 2)
+        pms, pinfo = timed(p_steps)
+        assert (rep.valid_kmers, rep.positive_estimates, rep.estimate_checksum) == fused_report
+        pvalue = all_kmers * p_steps / (pms / 1e3)
+        plain = {"value": pvalue, "unit": "k-mers/s", "ms_per_step": pms / p_steps,
+                 "insert_ms": pinfo["insert_ms"], "query_ms": pinfo["query_ms"],
+                 "batched_over_plain": value / pvalue}
+        check(L.scb_set_strategy(h, 2, 2))
+
+    e2e = None
+    if not args.no_e2e:
+        p_data = torch.from_numpy(data).pin_memory()
+        p_off = torch.from_numpy(offsets.view(np.int64)).pin_memory()
+        times = []
+        for i in range(args.warmup + args.steps):
+            check(L.scb_reset(h))
+            torch.cuda.synchronize()
+            dist.barrier()
+            t0 = time.perf_counter()
+            check(L.scb_build_and_stream_query(h, p_data.data_ptr(), p_off.data_ptr(), n_seqs, C.byref(km),
+                                               C.byref(sm), C.byref(rep)))
+            dt = time.perf_counter() - t0
+            if i >= args.warmup:
+                times.append(dist.max(dt))
+        assert (rep.valid_kmers, rep.positive_estimates, rep.estimate_checksum) == fused_report
+        e2e = {"value": all_kmers * len(times) / sum(times), "unit": "k-mers/s",
+               "h2d_bytes_per_step": n_bytes + (n_seqs + 1) * 8, "d2h_bytes_per_step": 2 * (16 * 8 + 4)}
+
+    # roofline of the dominant kernel (the insert tile kernel: one launch per step)
+    peak, peak_kind = measured_peaks()
+    ins_bytes = 64 * st.sectors + n_bytes // 4
+    q_bytes = 32 * st.sectors + n_bytes // 4
+    dom = "insert" if info["insert_ms"] >= info["query_ms"] else "query"
+    dom_ms = info[f"{dom}_ms"]
+    alg = ins_bytes if dom == "insert" else q_bytes
+    achieved = alg / (dom_ms / 1e3) / 1e9
+    traffic = profile_traffic()
+    roofline = {"bound": "hbm", "kernel": f"k_tiles<{dom}>", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_kind": peak_kind,
+                "traffic": (traffic["dram_bytes_per_kmer"] * kmers) if traffic else None,
+                "algorithmic_bytes": alg, "kernel_ms": dom_ms,
+                "sectors_per_superkmer": st.sectors / max(st.super_kmers, 1),
+                "super_kmers": st.super_kmers, "smers": st.smers}
+
+    cpu = None
+    if not args.no_cpu and dist.rank == 0 and dist.world == 1:
+        from oracle import oracle
+
+        n = min(CPU_SAMPLE_READS, n_seqs)
+        so = offsets[: n + 1].copy()
+        sd = data[: int(so[-1])]
+        threads = os.cpu_count() or 1
+        f = oracle.OracleFilter(oracle.make_config(GEOM["k"], GEOM["m"], GEOM["s"], GEOM["n_hashes"],
+                                                   GEOM["counter_bits"], GEOM["counter_slots_exponent"],
+                                                   GEOM["block_slots_exponent"], threads, 4096))
+        t0 = time.perf_counter()
+        r = f.port_build_and_stream_query(sd, so, threads=threads, queue=4096)
+        dt = time.perf_counter() - t0
+        f.close()
+        cpu = {"value": r["inserted_kmers"] / dt, "unit": "k-mers/s", "cores": threads, "kind": "port",
+               "sample": f"first {n} reads ({r['inserted_kmers']} k-mers), build + stream query, fresh table"}
+
+    if dist.rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "k-mers/s", "n_gpus": dist.world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u16", "data": "synthetic",
+            "config": {"workload": WORKLOAD + (f" (genome scale {args.scale})" if args.scale != 1.0 else ""),
+                       "reads": n_seqs, "bytes": n_bytes, "kmers_per_step": kmers,
+                       "l2": "inputs larger than L2 (2 GB of reads, 2 GiB table)",
+                       "parallelism": f"replicas x{dist.world}", "strategy": "fused"},
+            "insert_kmers_per_s": kmers / (info["insert_ms"] / 1e3),
+            "query_kmers_per_s": kmers / (info["query_ms"] / 1e3),
+            "stage_ms": {"pack": info["pack_ms"], "insert": info["insert_ms"], "query": info["query_ms"]},
+            "plain": plain, "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
+            "clocks": info["clocks"], "gpu_launches": info["launches"],
+        }
+        print(json.dumps(line), flush=True)
+    del d_data, d_off
+    ctx.close()
+
+
+def main():
+    args = parse()
+    dist = Dist(args.gpus)
+    try:
+        if args.impl == "reference":
+            run_reference(args, dist)
+        else:
+            run_ours(args, dist)
+    finally:
+        dist.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,202 @@
+/*
+ * scb.h -- C ABI of the B200 (sm_100a) SuperCountingBloom library (libscb_b200.so).
+ *
+ * The entry points are what a GPU backend inside the reference crate's public API
+ * (super-counting-bloom 0.1.0, src/api.rs) binds through `extern "C"`: plain pointers and
+ * sizes, no Rust, no torch types.  Each declaration cites the reference interface it replaces.
+ *
+ * Conventions
+ *   - Sequences are passed as one concatenated byte buffer `seqs` plus `n_seqs + 1` offsets
+ *     (sequence i is seqs[offsets[i] .. offsets[i+1])), exactly the records the reference's
+ *     workers receive (src/api.rs:621-674).  Bytes other than A/C/G/T (either case) split a
+ *     sequence into runs; runs shorter than k are skipped (src/api.rs:676-726, 929-931).
+ *   - `*_device` entry points take device pointers and a CUDA stream (cudaStream_t passed as
+ *     void*); all others take host pointers (pinned or pageable) and return after the result
+ *     is on the host.
+ *   - Every function returns an scb_status; on failure scb_last_error() gives a thread-local
+ *     message.  Status values map 1:1 onto SuperCountingBloomError (src/error.rs:4-12).
+ *   - The library owns device memory; the caller owns host buffers.  No callbacks.
+ *   - Query entry points on a frozen index are thread-safe (src/api.rs:278-286 runs them
+ *     from several threads); insert entry points need a single writer (&mut self).
+ */
+#ifndef SCB_H
+#define SCB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* src/error.rs:4-12 */
+typedef enum scb_status {
+    SCB_OK = 0,
+    SCB_ERR_INVALID_CONFIG = 1,       /* InvalidConfig(String) */
+    SCB_ERR_FASTX_OPEN = 2,           /* FastxOpen { path, message } */
+    SCB_ERR_INVALID_INDEX_FORMAT = 3, /* InvalidIndexFormat(String) */
+    SCB_ERR_CHANNEL_CLOSED = 4,       /* ChannelClosed(String) */
+    SCB_ERR_WORKER_PANIC = 5,         /* WorkerPanic(&'static str) */
+    SCB_ERR_INTERNAL_STATE = 6,       /* InternalState(String): CUDA errors, device status words */
+    SCB_ERR_IO = 7                    /* Io { path, message } */
+} scb_status;
+
+/* src/config.rs:20-31 (SuperCountingBloomConfig); counter_bits is CounterBits::as_u8. */
+typedef struct scb_config {
+    uint64_t k;
+    uint64_t m;
+    uint64_t s;
+    uint64_t n_hashes;
+    uint8_t counter_bits;           /* 8, 16 or 32 */
+    uint8_t counter_slots_exponent; /* total counters = 2^counter_slots_exponent */
+    uint8_t block_slots_exponent;   /* counters per block = 2^block_slots_exponent */
+    uint64_t threads;               /* carried into .scb (src/api.rs:478) */
+    uint64_t queue;                 /* carried into .scb (src/api.rs:479) */
+} scb_config;
+
+/* src/api.rs:20-27 (QueryFastaReport); also the stream-query statistics of
+ * src/fastx.rs:74-79 (queried_kmers = valid_kmers). */
+typedef struct scb_report {
+    uint64_t records_processed;
+    uint64_t total_windows;
+    uint64_t valid_kmers;
+    uint64_t positive_estimates;
+    uint64_t estimate_checksum; /* wrapping sum of the estimates */
+} scb_report;
+
+/* Device-side work statistics of a batch (super-k-mers, s-mers, distinct 32-byte sectors of
+ * the counter blocks touched per super-k-mer); used to state algorithmic bytes. */
+typedef struct scb_stats {
+    uint64_t windows;
+    uint64_t super_kmers;
+    uint64_t smers;
+    uint64_t sectors;
+} scb_stats;
+
+/* Insert / query kernel strategies (selected by the autotuner unless set). */
+typedef enum scb_strategy {
+    SCB_STRATEGY_AUTO = 0,
+    SCB_STRATEGY_PLAIN = 1,  /* one launch per stage, per-window arrays in HBM, direct atomics */
+    SCB_STRATEGY_FUSED = 2,  /* one persistent tile kernel over a device work queue */
+    SCB_STRATEGY_STAGED = 3, /* fused tiles, one warp per super-k-mer staging its block deltas */
+    SCB_STRATEGY_GROUPED = 4 /* super-k-mers bucketed by block, blocks applied in shared memory */
+} scb_strategy;
+
+typedef struct scb_ctx scb_ctx;
+
+/* Thread-local text of the last failure on this thread ("" if none). */
+const char* scb_last_error(void);
+/* Library version string. */
+const char* scb_version(void);
+
+/* src/config.rs:33-47 (Default).  threads is set to the host's core count. */
+scb_status scb_config_default(scb_config* cfg);
+/* src/config.rs:50-92 + src/filter.rs:96-100 (number of blocks a power of two). */
+scb_status scb_config_validate(const scb_config* cfg);
+
+/* SuperCountingBloomBuilder::new (src/api.rs:101-121): validates, allocates the counter table
+ * on device 0 (or the current device) in .scb file order and zeroes it. */
+scb_status scb_create(const scb_config* cfg, scb_ctx** out);
+/* Drop of builder / index: frees all device memory of the context. */
+void scb_destroy(scb_ctx* ctx);
+
+/* SuperCountingBloomBuilder::add_sequence / add_fasta's per-record insert
+ * (src/api.rs:123-158, 621-726, filter.rs:199-237).  Adds the batch's k-mer windows and
+ * inserted s-mers to the context totals and returns this batch's counts. */
+scb_status scb_insert_batch(scb_ctx* ctx, const uint8_t* seqs, const uint64_t* offsets, uint64_t n_seqs,
+                            uint64_t* inserted_kmers, uint64_t* inserted_smers);
+scb_status scb_insert_batch_device(scb_ctx* ctx, const uint8_t* d_seqs, const uint64_t* d_offsets,
+                                   uint64_t n_seqs, uint64_t n_bytes, void* stream,
+                                   uint64_t* inserted_kmers, uint64_t* inserted_smers);
+
+/* SuperCountingBloomBuilder::into_index (src/api.rs:160-177).  After freezing, inserts fail
+ * with SCB_ERR_INTERNAL_STATE and queries are allowed. */
+scb_status scb_freeze(scb_ctx* ctx);
+/* SuperCountingBloomBuilder::{inserted_kmers, inserted_smers}, SuperCountingBloomIndex::
+ * {inserted_kmers, config} (src/api.rs:179-207, 225-231). */
+scb_status scb_get_counts(const scb_ctx* ctx, uint64_t* inserted_kmers, uint64_t* inserted_smers);
+scb_status scb_get_config(const scb_ctx* ctx, scb_config* cfg);
+/* SuperCountingBloomBuilder::set_threads (src/api.rs:187-195): only the value carried into .scb. */
+scb_status scb_set_threads(scb_ctx* ctx, uint64_t threads);
+
+/* SuperCountingBloomIndex::estimate_sequence_abundances for each sequence
+ * (src/api.rs:250-262, 799-853).  Sequence i contributes max(0, len_i + 1 - k) windows,
+ * written consecutively; valid[w] = 0 marks a window with a non-ACGT base (None). */
+scb_status scb_query_batch(scb_ctx* ctx, const uint8_t* seqs, const uint64_t* offsets, uint64_t n_seqs,
+                           uint64_t* abundances, uint8_t* valid);
+scb_status scb_query_batch_device(scb_ctx* ctx, const uint8_t* d_seqs, const uint64_t* d_offsets,
+                                  uint64_t n_seqs, uint64_t n_bytes, void* stream, uint64_t* d_abundances,
+                                  uint8_t* d_valid);
+/* Number of windows scb_query_batch writes for these offsets. */
+uint64_t scb_count_windows(const scb_ctx* ctx, const uint64_t* offsets, uint64_t n_seqs);
+
+/* SuperCountingBloomIndex::query_fasta's reduction (src/api.rs:273-327): records, windows,
+ * valid k-mers, positive estimates and the wrapping checksum, without per-window output. */
+scb_status scb_query_report(scb_ctx* ctx, const uint8_t* seqs, const uint64_t* offsets, uint64_t n_seqs,
+                            scb_report* report);
+scb_status scb_query_report_device(scb_ctx* ctx, const uint8_t* d_seqs, const uint64_t* d_offsets,
+                                   uint64_t n_seqs, uint64_t n_bytes, void* stream, scb_report* report);
+
+/* stream_estimates_from_fastx (src/fastx.rs:107-131, 172-204, 206-253, 310-369) on in-memory
+ * records: builds from the records, freezes, then stream-queries the same records.  The
+ * records are copied to the device once and kept resident between the two passes. */
+scb_status scb_build_and_stream_query(scb_ctx* ctx, const uint8_t* seqs, const uint64_t* offsets,
+                                      uint64_t n_seqs, uint64_t* inserted_kmers, uint64_t* inserted_smers,
+                                      scb_report* report);
+
+/* estimate_distinct_kmers + spectrum_from_estimates (src/fastx.rs:255-308, 392-410): the
+ * histogram over distinct canonical k-mers of their estimates, rows sorted by value.  Call
+ * with values == NULL to get the row count in *n_rows; then call again with capacity >= rows.
+ * *distinct_keys = number of distinct canonical k-mers, *queried_kmers = windows queried. */
+scb_status scb_spectrum_distinct(scb_ctx* ctx, const uint8_t* seqs, const uint64_t* offsets, uint64_t n_seqs,
+                                 uint64_t* values, uint64_t* counts, uint64_t capacity, uint64_t* n_rows,
+                                 uint64_t* distinct_keys, uint64_t* queried_kmers);
+
+/* SuperCountingBloomIndex::counter_histogram (src/api.rs:329-335, filter.rs:267-275): value ->
+ * number of counters, rows sorted by value.  Same two-call convention as above. */
+scb_status scb_counter_histogram(scb_ctx* ctx, uint64_t* values, uint64_t* counts, uint64_t capacity,
+                                 uint64_t* n_rows);
+
+/* SuperCountingBloomIndex::save / load (src/api.rs:233-248, 388-608): the .scb file, byte
+ * identical to the reference's writer.  scb_load creates a frozen context. */
+scb_status scb_save(const scb_ctx* ctx, const char* path);
+scb_status scb_load(const char* path, scb_ctx** out);
+/* Raw counter table in file order (little-endian), for callers that do their own I/O
+ * (src/filter.rs:575-605). bytes must equal 2^counter_slots_exponent * counter_bits / 8. */
+uint64_t scb_table_bytes(const scb_ctx* ctx);
+scb_status scb_table_download(const scb_ctx* ctx, void* host, uint64_t bytes);
+scb_status scb_table_upload(scb_ctx* ctx, const void* host, uint64_t bytes, uint64_t inserted_kmers);
+
+/* Strategy control and workload statistics. */
+scb_status scb_set_strategy(scb_ctx* ctx, scb_strategy insert_strategy, scb_strategy query_strategy);
+scb_status scb_get_strategy(const scb_ctx* ctx, scb_strategy* insert_strategy, scb_strategy* query_strategy);
+scb_status scb_batch_stats(scb_ctx* ctx, const uint8_t* seqs, const uint64_t* offsets, uint64_t n_seqs,
+                           scb_stats* stats);
+/* Per-window chosen minimizer position, indexed by byte position of the batch (UINT32_MAX where
+ * no valid window starts): exposes kernel (b) alone for localising mismatches. */
+scb_status scb_debug_window_minimizers(scb_ctx* ctx, const uint8_t* seqs, const uint64_t* offsets,
+                                       uint64_t n_seqs, uint32_t* out);
+/* Number of kernels this library launched since load (all contexts). */
+uint64_t scb_kernel_launches(void);
+
+/* Per-stage device times (CUDA events on the launching stream), accumulated over batches
+ * since timing was enabled: pack = kernel (a) plus sequence starts; insert / query = the
+ * insert or query kernels of the active strategy (plain: the per-window stage included). */
+typedef struct scb_timings {
+    double pack_ms;
+    double insert_ms;
+    double query_ms;
+    uint64_t batches;
+} scb_timings;
+scb_status scb_set_timing(scb_ctx* ctx, int enable); /* enabling also clears the totals */
+scb_status scb_get_timings(const scb_ctx* ctx, scb_timings* out);
+
+/* Clears the counter table and the insert totals and makes the context a builder again
+ * (SuperCountingBloomBuilder::new on the existing allocation). */
+scb_status scb_reset(scb_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SCB_H */

@@ -1,0 +1,1094 @@
+// C ABI of the B200 SuperCountingBloom library: context lifecycle, batch staging, kernel
+// pipelines per strategy, .scb save/load.  See include/scb.h for the contract of each entry.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/scb.h"
+#include "scb_kernels.cuh"
+
+using namespace scb;
+
+// ---------------------------------------------------------------------------------------
+// Errors
+// ---------------------------------------------------------------------------------------
+namespace {
+
+thread_local std::string g_last_error;
+
+scb_status fail(scb_status st, const std::string& msg) {
+    g_last_error = msg;
+    return st;
+}
+
+const char* kind_prefix(scb_status st) {
+    switch (st) {
+        case SCB_ERR_INVALID_CONFIG: return "invalid config: ";
+        case SCB_ERR_INVALID_INDEX_FORMAT: return "invalid index format: ";
+        case SCB_ERR_INTERNAL_STATE: return "internal state error: ";
+        case SCB_ERR_IO: return "I/O error for ";
+        default: return "";
+    }
+}
+
+scb_status fail_kind(scb_status st, const std::string& msg) { return fail(st, std::string(kind_prefix(st)) + msg); }
+
+#define SCB_CUDA(call)                                                                               \
+    do {                                                                                             \
+        cudaError_t e_ = (call);                                                                     \
+        if (e_ != cudaSuccess) {                                                                     \
+            return fail_kind(SCB_ERR_INTERNAL_STATE, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+        }                                                                                            \
+    } while (0)
+
+#define SCB_TRY(expr)                 \
+    do {                              \
+        scb_status s_ = (expr);       \
+        if (s_ != SCB_OK) return s_;  \
+    } while (0)
+
+// ---------------------------------------------------------------------------------------
+// Device buffers
+// ---------------------------------------------------------------------------------------
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    ~DevBuf() {
+        if (p) cudaFree(p);
+    }
+    scb_status ensure(size_t bytes) {
+        if (bytes <= cap) return SCB_OK;
+        if (p) {
+            cudaFree(p);
+            p = nullptr;
+            cap = 0;
+        }
+        size_t want = std::max<size_t>(bytes, 256);
+        cudaError_t e = cudaMalloc(&p, want);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            return fail_kind(SCB_ERR_INTERNAL_STATE,
+                             "device allocation of " + std::to_string(want) + " bytes failed: " + cudaGetErrorString(e));
+        }
+        cap = want;
+        return SCB_OK;
+    }
+    template <typename T>
+    T* as() const {
+        return reinterpret_cast<T*>(p);
+    }
+};
+
+// Largest batch the kernels index with 32-bit positions.
+constexpr uint64_t kMaxBatchBytes = (1ull << 31);
+constexpr uint64_t kPadWords = 16;
+
+// Derived per-batch arrays (codes, bitmaps, window offsets, plain-pipeline arrays, counters).
+struct Lane {
+    DevBuf ascii, offsets, codes, valid, seqstart, woff, scan, wblock, wend, cnt, tiles;
+    cudaStream_t stream = nullptr;
+    // stage timing: [0,1] pack, [2,3] main stage; main_kind 1 = insert, 2 = query
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    bool pack_timed = false;
+    int main_kind = 0;
+    ~Lane() {
+        for (auto& e : ev) {
+            if (e) cudaEventDestroy(e);
+        }
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+}  // namespace
+
+struct scb_ctx {
+    scb_config cfg{};
+    DevGeom g{};
+    // FrozenFilterLayout (filter.rs:77-116)
+    uint64_t shard_count = 0, subblocks = 0, block_slots = 0, shard_mask = 0, block_slots_mask = 0, nb_blocks = 0,
+             block_mask = 0;
+    uint32_t shard_shift = 0;
+    int device = 0;
+    int sm_count = 148;
+    void* table = nullptr;
+    uint64_t table_bytes = 0;
+    uint32_t* status = nullptr;
+    bool frozen = false;
+    uint64_t inserted_kmers = 0, inserted_smers = 0;
+    scb_strategy insert_strategy = SCB_STRATEGY_AUTO, query_strategy = SCB_STRATEGY_AUTO;
+    Lane lane;
+    bool timing = false;
+    scb_timings times{};
+    std::mutex mu;
+    ~scb_ctx() {
+        if (table) cudaFree(table);
+        if (status) cudaFree(status);
+    }
+};
+
+namespace {
+
+uint32_t log2u(uint64_t v) {
+    uint32_t r = 0;
+    while ((1ull << r) < v) r++;
+    return r;
+}
+
+// config.rs:50-92 and filter.rs:96-100, with the reference's messages.
+scb_status validate_config(const scb_config* c) {
+    if (!c) return fail_kind(SCB_ERR_INVALID_CONFIG, "null config");
+    if (c->k == 0 || c->k > 32) return fail_kind(SCB_ERR_INVALID_CONFIG, "k must be in 1..=32");
+    if (c->m == 0 || c->m > c->k) return fail_kind(SCB_ERR_INVALID_CONFIG, "m must be in 1..=k");
+    if (c->s == 0 || c->s > c->k || c->s > 32) return fail_kind(SCB_ERR_INVALID_CONFIG, "s must be in 1..=k and <= 32");
+    if (c->k % 2 == 0) return fail_kind(SCB_ERR_INVALID_CONFIG, "canonical SIMD minimizers require odd k");
+    if (c->n_hashes == 0) return fail_kind(SCB_ERR_INVALID_CONFIG, "n_hashes must be positive");
+    if (c->block_slots_exponent >= c->counter_slots_exponent)
+        return fail_kind(SCB_ERR_INVALID_CONFIG, "block_slots_exponent must be smaller than counter_slots_exponent");
+    if (c->threads == 0) return fail_kind(SCB_ERR_INVALID_CONFIG, "threads must be positive");
+    if (c->queue == 0) return fail_kind(SCB_ERR_INVALID_CONFIG, "queue must be positive");
+    if (c->counter_bits != 8 && c->counter_bits != 16 && c->counter_bits != 32)
+        return fail_kind(SCB_ERR_INVALID_CONFIG, "unsupported counter width");
+    if (c->counter_slots_exponent >= 64) return fail_kind(SCB_ERR_INVALID_CONFIG, "counter_slots_exponent is too large");
+    return SCB_OK;
+}
+
+// Device limits of this implementation (beyond the reference's rules).
+scb_status device_limits(const scb_config* c) {
+    if (c->counter_slots_exponent - c->block_slots_exponent > 32)
+        return fail_kind(SCB_ERR_INVALID_CONFIG, "more than 2^32 blocks is beyond the device table limit");
+    if (c->counter_slots_exponent > 37)
+        return fail_kind(SCB_ERR_INVALID_CONFIG, "counter_slots_exponent above 37 exceeds device memory");
+    return SCB_OK;
+}
+
+void fill_geometry(scb_ctx* ctx) {
+    const scb_config& c = ctx->cfg;
+    const uint64_t slots = 1ull << c.counter_slots_exponent;
+    ctx->block_slots = 1ull << c.block_slots_exponent;
+    ctx->nb_blocks = slots / ctx->block_slots;
+    ctx->shard_count = std::min<uint64_t>(ctx->nb_blocks, 1024);
+    ctx->subblocks = ctx->nb_blocks / ctx->shard_count;
+    ctx->shard_mask = ctx->shard_count - 1;
+    ctx->shard_shift = log2u(ctx->shard_count);
+    ctx->block_slots_mask = ctx->block_slots - 1;
+    ctx->block_mask = ctx->nb_blocks - 1;
+    ctx->table_bytes = slots * (c.counter_bits / 8);
+    DevGeom& g = ctx->g;
+    g.k = (uint32_t)c.k;
+    g.m = (uint32_t)c.m;
+    g.s = (uint32_t)c.s;
+    g.h = (uint32_t)c.n_hashes;
+    g.w = (uint32_t)(c.k - c.m + 1);
+    g.bits = c.counter_bits;
+    g.block_log2 = c.block_slots_exponent;
+    g.shard_shift = ctx->shard_shift;
+    g.sub_log2 = log2u(ctx->subblocks);
+    g.block_mask = ctx->block_mask;
+    g.shard_mask = ctx->shard_mask;
+    g.bs_mask = ctx->block_slots_mask;
+}
+
+scb_status check_offsets(const uint64_t* offsets, uint64_t n) {
+    if (!offsets) return fail_kind(SCB_ERR_INTERNAL_STATE, "null offsets");
+    for (uint64_t i = 0; i < n; i++) {
+        if (offsets[i + 1] < offsets[i]) return fail_kind(SCB_ERR_INTERNAL_STATE, "offsets must be non-decreasing");
+    }
+    return SCB_OK;
+}
+
+uint64_t windows_of(const uint64_t* offsets, uint64_t n, uint64_t k) {
+    uint64_t w = 0;
+    for (uint64_t i = 0; i < n; i++) {
+        const uint64_t len = offsets[i + 1] - offsets[i];
+        if (len >= k) w += len + 1 - k;
+    }
+    return w;
+}
+
+// A contiguous range of whole sequences processed as one device batch.
+struct Chunk {
+    uint64_t seq0, seq1;    // sequences [seq0, seq1)
+    uint64_t byte0, byte1;  // bytes [byte0, byte1) of the caller's buffer
+    uint64_t win0;          // first output window of the chunk
+};
+
+scb_status plan_chunks(const uint64_t* offsets, uint64_t n, uint64_t k, uint64_t cap, std::vector<Chunk>& out) {
+    out.clear();
+    uint64_t s = 0, win = 0;
+    while (s < n) {
+        uint64_t e = s;
+        const uint64_t b0 = offsets[s];
+        uint64_t w = 0;
+        while (e < n && (e == s || offsets[e + 1] - b0 <= cap)) {
+            const uint64_t len = offsets[e + 1] - offsets[e];
+            w += len >= k ? len + 1 - k : 0;
+            e++;
+        }
+        if (offsets[e] - b0 > kMaxBatchBytes - 64)
+            return fail_kind(SCB_ERR_INTERNAL_STATE, "a single sequence longer than 2 GiB is not supported");
+        out.push_back(Chunk{s, e, b0, offsets[e], win});
+        win += w;
+        s = e;
+    }
+    return SCB_OK;
+}
+
+__global__ void k_rebase(uint64_t* off, uint64_t n, uint64_t base) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) off[i] -= base;
+}
+
+scb_status ensure_lane(scb_ctx* ctx, Lane& L, uint64_t n_bytes, uint64_t n_seqs) {
+    if (!L.stream) SCB_CUDA(cudaStreamCreateWithFlags(&L.stream, cudaStreamNonBlocking));
+    const uint64_t groups = (n_bytes + 31) / 32;
+    SCB_TRY(L.ascii.ensure(groups * 32 + 64));
+    SCB_TRY(L.offsets.ensure((n_seqs + 1) * 8));
+    SCB_TRY(L.codes.ensure((2 * groups + kPadWords) * 4));
+    SCB_TRY(L.valid.ensure((groups + kPadWords) * 4));
+    SCB_TRY(L.seqstart.ensure((groups + kPadWords) * 4));
+    SCB_TRY(L.cnt.ensure(kCntSlots * 8));
+    SCB_TRY(L.tiles.ensure(64));
+    (void)ctx;
+    return SCB_OK;
+}
+
+// Stages a device batch (ascii + rebased offsets already on the device in L) into codes,
+// bitmaps and sequence starts, and fills the tile arguments.
+scb_status prepare_batch(scb_ctx* ctx, Lane& L, const uint8_t* d_ascii, const uint64_t* d_offsets, uint64_t n_seqs,
+                         uint64_t n_bytes, cudaStream_t st, TileArgs& a) {
+    const uint64_t groups = (n_bytes + 31) / 32;
+    if (ctx->timing) SCB_CUDA(cudaEventRecord(L.ev[0], st));
+    SCB_CUDA(cudaMemsetAsync(L.codes.p, 0, (2 * groups + kPadWords) * 4, st));
+    SCB_CUDA(cudaMemsetAsync(L.valid.p, 0, (groups + kPadWords) * 4, st));
+    SCB_CUDA(cudaMemsetAsync(L.seqstart.p, 0, (groups + kPadWords) * 4, st));
+    launch_pack(d_ascii, n_bytes, L.codes.as<uint32_t>(), L.valid.as<uint32_t>(), st);
+    launch_seqstart(d_offsets, n_seqs, n_bytes, L.seqstart.as<uint32_t>(), st);
+    if (ctx->timing) {
+        SCB_CUDA(cudaEventRecord(L.ev[1], st));
+        L.pack_timed = true;
+    }
+    SCB_CUDA(cudaMemsetAsync(L.cnt.p, 0, kCntSlots * 8, st));
+    std::memset(&a, 0, sizeof(a));
+    a.g = ctx->g;
+    a.codes = L.codes.as<uint32_t>();
+    a.valid = L.valid.as<uint32_t>();
+    a.seqstart = L.seqstart.as<uint32_t>();
+    a.n_bytes = n_bytes;
+    a.n_code_words = 2 * groups;
+    a.n_bit_words = groups;
+    a.n_tiles = (uint32_t)((n_bytes + kTileWindows - 1) / kTileWindows);
+    a.table = ctx->table;
+    a.status = ctx->status;
+    a.cnt = L.cnt.as<unsigned long long>();
+    a.tile_counter = L.tiles.as<unsigned int>();
+    a.offsets = d_offsets;
+    a.n_seqs = n_seqs;
+    return SCB_OK;
+}
+
+scb_strategy resolve(scb_strategy s) {
+    if (s == SCB_STRATEGY_PLAIN) return SCB_STRATEGY_PLAIN;
+    return SCB_STRATEGY_FUSED;
+}
+
+scb_status run_tiles(scb_ctx* ctx, Lane& L, int mode, TileArgs& a, cudaStream_t st) {
+    if (a.n_tiles == 0) return SCB_OK;
+    SCB_CUDA(cudaMemsetAsync(L.tiles.p, 0, 4, st));
+    const int grid = tile_grid(mode, ctx->g.bits, ctx->sm_count, a.n_tiles);
+    launch_tiles(mode, a, grid, st);
+    SCB_CUDA(cudaGetLastError());
+    return SCB_OK;
+}
+
+// Plain pipeline stage (b): per-window block ids and end flags in HBM.
+scb_status run_materialize(scb_ctx* ctx, Lane& L, TileArgs& a, cudaStream_t st) {
+    SCB_TRY(L.wblock.ensure(std::max<uint64_t>(a.n_bytes, 1) * 4));
+    SCB_TRY(L.wend.ensure(std::max<uint64_t>(a.n_bytes, 1)));
+    a.wblock = L.wblock.as<uint32_t>();
+    a.wend = L.wend.as<uint8_t>();
+    return run_tiles(ctx, L, kModeMaterialize, a, st);
+}
+
+scb_status insert_stage(scb_ctx* ctx, Lane& L, TileArgs& a, cudaStream_t st) {
+    if (resolve(ctx->insert_strategy) == SCB_STRATEGY_PLAIN) {
+        SCB_TRY(run_materialize(ctx, L, a, st));
+        launch_plain_insert(a, st);
+        SCB_CUDA(cudaGetLastError());
+        return SCB_OK;
+    }
+    return run_tiles(ctx, L, kModeInsert, a, st);
+}
+
+scb_status query_stage(scb_ctx* ctx, Lane& L, int mode, TileArgs& a, cudaStream_t st) {
+    if (resolve(ctx->query_strategy) == SCB_STRATEGY_PLAIN && (mode == kModeReport || mode == kModeAbund)) {
+        SCB_TRY(run_materialize(ctx, L, a, st));
+        launch_plain_query(mode, a, st);
+        SCB_CUDA(cudaGetLastError());
+        return SCB_OK;
+    }
+    return run_tiles(ctx, L, mode, a, st);
+}
+
+// The insert / query stage between two timing events when timing is on.
+scb_status insert_device_batch(scb_ctx* ctx, Lane& L, TileArgs& a, cudaStream_t st) {
+    if (ctx->timing) SCB_CUDA(cudaEventRecord(L.ev[2], st));
+    SCB_TRY(insert_stage(ctx, L, a, st));
+    if (ctx->timing) {
+        SCB_CUDA(cudaEventRecord(L.ev[3], st));
+        L.main_kind = 1;
+    }
+    return SCB_OK;
+}
+
+scb_status query_device_batch(scb_ctx* ctx, Lane& L, int mode, TileArgs& a, cudaStream_t st) {
+    if (ctx->timing) SCB_CUDA(cudaEventRecord(L.ev[2], st));
+    SCB_TRY(query_stage(ctx, L, mode, a, st));
+    if (ctx->timing) {
+        SCB_CUDA(cudaEventRecord(L.ev[3], st));
+        L.main_kind = 2;
+    }
+    return SCB_OK;
+}
+
+scb_status read_counters(scb_ctx* ctx, Lane& L, cudaStream_t st, unsigned long long* host) {
+    SCB_CUDA(cudaMemcpyAsync(host, L.cnt.p, kCntSlots * 8, cudaMemcpyDeviceToHost, st));
+    uint32_t status = 0;
+    SCB_CUDA(cudaMemcpyAsync(&status, ctx->status, 4, cudaMemcpyDeviceToHost, st));
+    SCB_CUDA(cudaStreamSynchronize(st));
+    if (ctx->timing) {
+        float ms = 0;
+        if (L.pack_timed && cudaEventElapsedTime(&ms, L.ev[0], L.ev[1]) == cudaSuccess) ctx->times.pack_ms += ms;
+        if (L.main_kind && cudaEventElapsedTime(&ms, L.ev[2], L.ev[3]) == cudaSuccess) {
+            (L.main_kind == 1 ? ctx->times.insert_ms : ctx->times.query_ms) += ms;
+        }
+        if (L.pack_timed || L.main_kind) ctx->times.batches++;
+        L.pack_timed = false;
+        L.main_kind = 0;
+    }
+    if (status) {
+        return fail_kind(SCB_ERR_INTERNAL_STATE, "device status word 0x" + std::to_string(status) +
+                                                     " (1=CAS retry limit, 2=distinct set full, 4=overflow list full)");
+    }
+    return SCB_OK;
+}
+
+// Copies a host chunk into the lane and rebases its offsets.
+scb_status upload_chunk(scb_ctx* ctx, Lane& L, const uint8_t* seqs, const uint64_t* offsets, const Chunk& c) {
+    const uint64_t n_seqs = c.seq1 - c.seq0, n_bytes = c.byte1 - c.byte0;
+    SCB_TRY(ensure_lane(ctx, L, n_bytes, n_seqs));
+    cudaStream_t st = L.stream;
+    if (n_bytes) SCB_CUDA(cudaMemcpyAsync(L.ascii.p, seqs + c.byte0, n_bytes, cudaMemcpyHostToDevice, st));
+    SCB_CUDA(cudaMemcpyAsync(L.offsets.p, offsets + c.seq0, (n_seqs + 1) * 8, cudaMemcpyHostToDevice, st));
+    if (c.byte0) {
+        k_rebase<<<(unsigned)((n_seqs + 1 + 255) / 256), 256, 0, st>>>(L.offsets.as<uint64_t>(), n_seqs + 1, c.byte0);
+        note_launch();
+    }
+    return SCB_OK;
+}
+
+struct CtxLock {
+    std::unique_lock<std::mutex> lk;
+    explicit CtxLock(scb_ctx* c) : lk(c->mu) { cudaSetDevice(c->device); }
+};
+
+scb_status alloc_ctx(const scb_config* cfg, scb_ctx** out) {
+    SCB_TRY(validate_config(cfg));
+    SCB_TRY(device_limits(cfg));
+    int dev_count = 0;
+    cudaError_t e = cudaGetDeviceCount(&dev_count);
+    if (e != cudaSuccess || dev_count == 0) {
+        return fail_kind(SCB_ERR_INTERNAL_STATE, std::string("no CUDA device available: ") +
+                                                     (e != cudaSuccess ? cudaGetErrorString(e) : "0 devices"));
+    }
+    auto* ctx = new scb_ctx();
+    ctx->cfg = *cfg;
+    fill_geometry(ctx);
+    cudaGetDevice(&ctx->device);
+    cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, ctx->device);
+    // whole 32-bit words: counters are updated through 32-bit CAS on their containing word
+    e = cudaMalloc(&ctx->table, ((ctx->table_bytes + 255) / 256) * 256);
+    if (e != cudaSuccess) {
+        ctx->table = nullptr;
+        delete ctx;
+        return fail_kind(SCB_ERR_INTERNAL_STATE, "device allocation of the counter table failed: " +
+                                                     std::string(cudaGetErrorString(e)));
+    }
+    e = cudaMalloc(&ctx->status, 64);
+    if (e == cudaSuccess) e = cudaMemset(ctx->table, 0, ((ctx->table_bytes + 255) / 256) * 256);
+    if (e == cudaSuccess) e = cudaMemset(ctx->status, 0, 64);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+        delete ctx;
+        return fail_kind(SCB_ERR_INTERNAL_STATE, std::string("device setup failed: ") + cudaGetErrorString(e));
+    }
+    *out = ctx;
+    return SCB_OK;
+}
+
+// Host-pointer batch driver: runs fn(ctx, lane, tile_args, chunk) on every chunk.
+template <typename Fn>
+scb_status for_each_chunk(scb_ctx* ctx, const uint8_t* seqs, const uint64_t* offsets, uint64_t n, Fn&& fn) {
+    SCB_TRY(check_offsets(offsets, n));
+    std::vector<Chunk> chunks;
+    SCB_TRY(plan_chunks(offsets, n, ctx->cfg.k, kMaxBatchBytes - 64, chunks));
+    for (const Chunk& c : chunks) {
+        Lane& L = ctx->lane;
+        SCB_TRY(upload_chunk(ctx, L, seqs, offsets, c));
+        TileArgs a;
+        SCB_TRY(prepare_batch(ctx, L, L.ascii.as<uint8_t>(), L.offsets.as<uint64_t>(), c.seq1 - c.seq0,
+                              c.byte1 - c.byte0, L.stream, a));
+        SCB_TRY(fn(L, a, c));
+    }
+    return SCB_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------------------
+extern "C" {
+
+const char* scb_last_error(void) { return g_last_error.c_str(); }
+const char* scb_version(void) { return "scb_b200 0.1.0 (sm_100a)"; }
+uint64_t scb_kernel_launches(void) { return kernel_launch_count(); }
+
+scb_status scb_config_default(scb_config* cfg) {
+    if (!cfg) return fail_kind(SCB_ERR_INVALID_CONFIG, "null config");
+    cfg->k = 31;
+    cfg->m = 21;
+    cfg->s = 25;
+    cfg->n_hashes = 4;
+    cfg->counter_bits = 16;
+    cfg->counter_slots_exponent = 30;
+    cfg->block_slots_exponent = 9;
+    const unsigned hc = std::thread::hardware_concurrency();
+    cfg->threads = hc ? hc : 1;
+    cfg->queue = 4096;
+    return SCB_OK;
+}
+
+scb_status scb_config_validate(const scb_config* cfg) { return validate_config(cfg); }
+
+scb_status scb_create(const scb_config* cfg, scb_ctx** out) {
+    if (!out) return fail_kind(SCB_ERR_INTERNAL_STATE, "null output pointer");
+    *out = nullptr;
+    return alloc_ctx(cfg, out);
+}
+
+void scb_destroy(scb_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    cudaDeviceSynchronize();
+    delete ctx;
+}
+
+scb_status scb_get_counts(const scb_ctx* ctx, uint64_t* kmers, uint64_t* smers) {
+    if (!ctx) return fail_kind(SCB_ERR_INTERNAL_STATE, "null context");
+    if (kmers) *kmers = ctx->inserted_kmers;
+    if (smers) *smers = ctx->inserted_smers;
+    return SCB_OK;
+}
+
+scb_status scb_get_config(const scb_ctx* ctx, scb_config* cfg) {
+    if (!ctx || !cfg) return fail_kind(SCB_ERR_INTERNAL_STATE, "null argument");
+    *cfg = ctx->cfg;
+    return SCB_OK;
+}
+
+scb_status scb_set_threads(scb_ctx* ctx, uint64_t threads) {
+    if (!ctx) return fail_kind(SCB_ERR_INTERNAL_STATE, "null context");
+    if (threads == 0) return fail_kind(SCB_ERR_INVALID_CONFIG, "threads must be positive");
+    ctx->cfg.threads = threads;
+    return SCB_OK;
+}
+
+scb_status scb_freeze(scb_ctx* ctx) {
+    if (!ctx) return fail_kind(SCB_ERR_INTERNAL_STATE, "null context");
+    CtxLock lk(ctx);
+    SCB_CUDA(cudaDeviceSynchronize());
+    ctx->frozen = true;
+    return SCB_OK;
+}
+
+scb_status scb_set_strategy(scb_ctx* ctx, scb_strategy ins, scb_strategy q) {
+    if (!ctx) return fail_kind(SCB_ERR_INTERNAL_STATE, "null context");
+    ctx->insert_strategy = ins;
+    ctx->query_strategy = q;
+    return SCB_OK;
+}
+
+scb_status scb_get_strategy(const scb_ctx* ctx, scb_strategy* ins, scb_strategy* q) {
+    if (!ctx) return fail_kind(SCB_ERR_INTERNAL_STATE, "null context");
+    if (ins) *ins = resolve(ctx->insert_strategy);
+    if (q) *q = resolve(ctx->query_strategy);
+    return SCB_OK;
+}
+
+uint64_t scb_count_windows(const scb_ctx* ctx, const uint64_t* offsets, uint64_t n) {
+    if (!ctx || !offsets) return 0;
+    return windows_of(offsets, n, ctx->cfg.k);
+}
+
+scb_status scb_insert_batch(scb_ctx* ctx, const uint8_t* seqs, const uint64_t* offsets, uint64_t n,
+                            uint64_t* kmers, uint64_t* smers) {
+    if (!ctx) return fail_kind(SCB_ERR_INTERNAL_STATE, "null context");
+    CtxLock lk(ctx);
+    if (ctx->frozen) return fail_kind(SCB_ERR_INTERNAL_STATE, "the index is frozen; inserts need a builder");
+    uint64_t tk = 0, ts = 0;
+    SCB_TRY(for_each_chunk(ctx, seqs, offsets, n, [&](Lane& L, TileArgs& a, const Chunk&) -> scb_status {
+        SCB_TRY(insert_device_batch(ctx, L, a, L.stream));
+        unsigned long long c[kCntSlots];
+        SCB_TRY(read_counters(ctx, L, L.stream, c));
+        tk += c[kCntWindows];
+        ts += c[kCntSmers];
+        return SCB_OK;
+    }));
+    ctx->inserted_kmers += tk;
+    ctx->inserted_smers += ts;
+    if (kmers) *kmers = tk;
+    if (smers) *smers = ts;
+    return SCB_OK;
+}
+
+scb_status scb_insert_batch_device(scb_ctx* ctx, const uint8_t* d_seqs, const uint64_t* d_offsets, uint64_t n,
+                                   uint64_t n_bytes, void* stream, uint64_t* kmers, uint64_t* smers) {
+    if (!ctx) return fail_kind(SCB_ERR_INTERNAL_STATE, "null context");
+    CtxLock lk(ctx);
+    if (ctx->frozen) return fail_kind(SCB_ERR_INTERNAL_STATE, "the index is frozen; inserts need a builder");
+    if (n_bytes > kMaxBatchBytes - 64) return fail_kind(SCB_ERR_INTERNAL_STATE, "device batch above 2 GiB");
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    Lane& L = ctx->lane;
+    SCB_TRY(ensure_lane(ctx, L, n_bytes, n));
+    TileArgs a;
+    SCB_TRY(prepare_batch(ctx, L, d_seqs, d_offsets, n, n_bytes, st, a));
+    SCB_TRY(insert_device_batch(ctx, L, a, st));
+    unsigned long long c[kCntSlots];
+    SCB_TRY(read_counters(ctx, L, st, c));
+    ctx->inserted_kmers += c[kCntWindows];
+    ctx->inserted_smers += c[kCntSmers];
+    if (kmers) *kmers = c[kCntWindows];
+    if (smers) *smers = c[kCntSmers];
+    return SCB_OK;
+}
+
+static scb_status need_frozen(const scb_ctx* ctx) {
+    if (!ctx) return fail_kind(SCB_ERR_INTERNAL_STATE, "null context");
+    if (!ctx->frozen) return fail_kind(SCB_ERR_INTERNAL_STATE, "queries need a frozen index (into_index)");
+    return SCB_OK;
+}
+
+scb_status scb_query_report(scb_ctx* ctx, const uint8_t* seqs, const uint64_t* offsets, uint64_t n,
+                            scb_report* rep) {
+    SCB_TRY(need_frozen(ctx));
+    if (!rep) return fail_kind(SCB_ERR_INTERNAL_STATE, "null report");
+    CtxLock lk(ctx);
+    std::memset(rep, 0, sizeof(*rep));
+    SCB_TRY(for_each_chunk(ctx, seqs, offsets, n, [&](Lane& L, TileArgs& a, const Chunk& ch) -> scb_status {
+        launch_seq_windows(a.offsets, ch.seq1 - ch.seq0, ctx->g.k, a.cnt, nullptr, L.stream);
+        SCB_TRY(query_device_batch(ctx, L, kModeReport, a, L.stream));
+        unsigned long long c[kCntSlots];
+        SCB_TRY(read_counters(ctx, L, L.stream, c));
+        rep->records_processed += c[kCntRecords];
+        rep->total_windows += c[kCntTotalWindows];
+        rep->valid_kmers += c[kCntValid];
+        rep->positive_estimates += c[kCntPositive];
+        rep->estimate_checksum += c[kCntChecksum];
+        return SCB_OK;
+    }));
+    return SCB_OK;
+}
+
+scb_status scb_query_report_device(scb_ctx* ctx, const uint8_t* d_seqs, const uint64_t* d_offsets, uint64_t n,
+                                   uint64_t n_bytes, void* stream, scb_report* rep) {
+    SCB_TRY(need_frozen(ctx));
+    if (!rep) return fail_kind(SCB_ERR_INTERNAL_STATE, "null report");
+    CtxLock lk(ctx);
+    if (n_bytes > kMaxBatchBytes - 64) return fail_kind(SCB_ERR_INTERNAL_STATE, "device batch above 2 GiB");
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    Lane& L = ctx->lane;
+    SCB_TRY(ensure_lane(ctx, L, n_bytes, n));
+    TileArgs a;
+    SCB_TRY(prepare_batch(ctx, L, d_seqs, d_offsets, n, n_bytes, st, a));
+    launch_seq_windows(d_offsets, n, ctx->g.k, a.cnt, nullptr, st);
+    SCB_TRY(query_device_batch(ctx, L, kModeReport, a, st));
+    unsigned long long c[kCntSlots];
+    SCB_TRY(read_counters(ctx, L, st, c));
+    rep->records_processed = c[kCntRecords];
+    rep->total_windows = c[kCntTotalWindows];
+    rep->valid_kmers = c[kCntValid];
+    rep->positive_estimates = c[kCntPositive];
+    rep->estimate_checksum = c[kCntChecksum];
+    return SCB_OK;
+}
+
+// Per-window abundances of one device batch into d_out / d_valid (windows of the batch).
+static scb_status abund_batch(scb_ctx* ctx, Lane& L, TileArgs& a, uint64_t n_seqs, cudaStream_t st,
+                              unsigned long long* d_out, uint8_t* d_valid, uint64_t n_windows) {
+    SCB_TRY(L.woff.ensure((n_seqs + 1) * 8));
+    SCB_TRY(L.scan.ensure(((n_seqs + 1) / 1024 + 64) * 8 * 2));
+    launch_seq_windows(a.offsets, n_seqs, ctx->g.k, a.cnt, L.woff.as<uint64_t>(), st);
+    launch_scan_inplace(L.woff.as<uint64_t>(), n_seqs, L.scan.as<uint64_t>(), st);
+    if (n_windows) {
+        SCB_CUDA(cudaMemsetAsync(d_out, 0, n_windows * 8, st));
+        SCB_CUDA(cudaMemsetAsync(d_valid, 0, n_windows, st));
+    }
+    a.woff = L.woff.as<uint64_t>();
+    a.out = d_out;
+    a.out_valid = d_valid;
+    return query_device_batch(ctx, L, kModeAbund, a, st);
+}
+
+scb_status scb_query_batch(scb_ctx* ctx, const uint8_t* seqs, const uint64_t* offsets, uint64_t n, uint64_t* ab,
+                           uint8_t* valid) {
+    SCB_TRY(need_frozen(ctx));
+    CtxLock lk(ctx);
+    DevBuf d_out, d_valid;
+    SCB_TRY(for_each_chunk(ctx, seqs, offsets, n, [&](Lane& L, TileArgs& a, const Chunk& ch) -> scb_status {
+        const uint64_t nw = windows_of(offsets + ch.seq0, ch.seq1 - ch.seq0, ctx->cfg.k);
+        SCB_TRY(d_out.ensure(std::max<uint64_t>(nw, 1) * 8));
+        SCB_TRY(d_valid.ensure(std::max<uint64_t>(nw, 1)));
+        SCB_TRY(abund_batch(ctx, L, a, ch.seq1 - ch.seq0, L.stream, d_out.as<unsigned long long>(),
+                            d_valid.as<uint8_t>(), nw));
+        if (nw) {
+            SCB_CUDA(cudaMemcpyAsync(ab + ch.win0, d_out.p, nw * 8, cudaMemcpyDeviceToHost, L.stream));
+            SCB_CUDA(cudaMemcpyAsync(valid + ch.win0, d_valid.p, nw, cudaMemcpyDeviceToHost, L.stream));
+        }
+        unsigned long long c[kCntSlots];
+        return read_counters(ctx, L, L.stream, c);
+    }));
+    return SCB_OK;
+}
+
+scb_status scb_query_batch_device(scb_ctx* ctx, const uint8_t* d_seqs, const uint64_t* d_offsets, uint64_t n,
+                                  uint64_t n_bytes, void* stream, uint64_t* d_ab, uint8_t* d_valid) {
+    SCB_TRY(need_frozen(ctx));
+    CtxLock lk(ctx);
+    if (n_bytes > kMaxBatchBytes - 64) return fail_kind(SCB_ERR_INTERNAL_STATE, "device batch above 2 GiB");
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    Lane& L = ctx->lane;
+    SCB_TRY(ensure_lane(ctx, L, n_bytes, n));
+    TileArgs a;
+    SCB_TRY(prepare_batch(ctx, L, d_seqs, d_offsets, n, n_bytes, st, a));
+    // window count: the scan's last element + last length is computed on the device; the
+    // caller sized the outputs with scb_count_windows, so clear through the kernel writes only
+    SCB_TRY(L.woff.ensure((n + 1) * 8));
+    SCB_TRY(L.scan.ensure(((n + 1) / 1024 + 64) * 8 * 2));
+    launch_seq_windows(d_offsets, n, ctx->g.k, a.cnt, L.woff.as<uint64_t>(), st);
+    launch_scan_inplace(L.woff.as<uint64_t>(), n, L.scan.as<uint64_t>(), st);
+    a.woff = L.woff.as<uint64_t>();
+    a.out = reinterpret_cast<unsigned long long*>(d_ab);
+    a.out_valid = d_valid;
+    SCB_TRY(query_device_batch(ctx, L, kModeAbund, a, st));
+    unsigned long long c[kCntSlots];
+    return read_counters(ctx, L, st, c);
+}
+
+scb_status scb_build_and_stream_query(scb_ctx* ctx, const uint8_t* seqs, const uint64_t* offsets, uint64_t n,
+                                      uint64_t* kmers, uint64_t* smers, scb_report* rep) {
+    if (!ctx || !rep) return fail_kind(SCB_ERR_INTERNAL_STATE, "null argument");
+    {
+        CtxLock lk(ctx);
+        if (ctx->frozen) return fail_kind(SCB_ERR_INTERNAL_STATE, "the index is frozen; inserts need a builder");
+        SCB_TRY(check_offsets(offsets, n));
+        const uint64_t total = n ? offsets[n] - offsets[0] : 0;
+        if (total <= kMaxBatchBytes - 64) {
+            // one resident batch: copy once, insert, freeze, query the same staged codes
+            Lane& L = ctx->lane;
+            Chunk c{0, n, n ? offsets[0] : 0, n ? offsets[n] : 0, 0};
+            SCB_TRY(upload_chunk(ctx, L, seqs, offsets, c));
+            TileArgs a;
+            SCB_TRY(prepare_batch(ctx, L, L.ascii.as<uint8_t>(), L.offsets.as<uint64_t>(), n, total, L.stream, a));
+            SCB_TRY(insert_device_batch(ctx, L, a, L.stream));
+            unsigned long long c1[kCntSlots];
+            SCB_TRY(read_counters(ctx, L, L.stream, c1));
+            ctx->inserted_kmers += c1[kCntWindows];
+            ctx->inserted_smers += c1[kCntSmers];
+            ctx->frozen = true;
+            SCB_CUDA(cudaMemsetAsync(L.cnt.p, 0, kCntSlots * 8, L.stream));
+            launch_seq_windows(a.offsets, n, ctx->g.k, a.cnt, nullptr, L.stream);
+            SCB_TRY(query_device_batch(ctx, L, kModeReport, a, L.stream));
+            unsigned long long c2[kCntSlots];
+            SCB_TRY(read_counters(ctx, L, L.stream, c2));
+            if (kmers) *kmers = c1[kCntWindows];
+            if (smers) *smers = c1[kCntSmers];
+            rep->records_processed = c2[kCntRecords];
+            rep->total_windows = c2[kCntTotalWindows];
+            rep->valid_kmers = c2[kCntValid];
+            rep->positive_estimates = c2[kCntPositive];
+            rep->estimate_checksum = c2[kCntChecksum];
+            return SCB_OK;
+        }
+    }
+    SCB_TRY(scb_insert_batch(ctx, seqs, offsets, n, kmers, smers));
+    SCB_TRY(scb_freeze(ctx));
+    return scb_query_report(ctx, seqs, offsets, n, rep);
+}
+
+// Rows of a dense histogram plus an overflow list, sorted by value, zero counts dropped.
+static void rows_from_hist(const std::vector<unsigned long long>& dense, std::vector<unsigned long long> ovf,
+                           std::vector<std::pair<uint64_t, uint64_t>>& rows) {
+    rows.clear();
+    for (size_t v = 0; v < dense.size(); v++) {
+        if (dense[v]) rows.emplace_back(v, dense[v]);
+    }
+    std::sort(ovf.begin(), ovf.end());
+    for (size_t i = 0; i < ovf.size();) {
+        size_t j = i;
+        while (j < ovf.size() && ovf[j] == ovf[i]) j++;
+        rows.emplace_back(ovf[i], j - i);
+        i = j;
+    }
+}
+
+static scb_status emit_rows(const std::vector<std::pair<uint64_t, uint64_t>>& rows, uint64_t* values, uint64_t* counts,
+                            uint64_t cap, uint64_t* n_rows) {
+    if (n_rows) *n_rows = rows.size();
+    if (!values || !counts) return SCB_OK;
+    if (cap < rows.size()) return fail_kind(SCB_ERR_INTERNAL_STATE, "row capacity too small");
+    for (size_t i = 0; i < rows.size(); i++) {
+        values[i] = rows[i].first;
+        counts[i] = rows[i].second;
+    }
+    return SCB_OK;
+}
+
+scb_status scb_spectrum_distinct(scb_ctx* ctx, const uint8_t* seqs, const uint64_t* offsets, uint64_t n,
+                                 uint64_t* values, uint64_t* counts, uint64_t capacity, uint64_t* n_rows,
+                                 uint64_t* distinct_keys, uint64_t* queried_kmers) {
+    SCB_TRY(need_frozen(ctx));
+    CtxLock lk(ctx);
+    SCB_TRY(check_offsets(offsets, n));
+    const uint64_t W = windows_of(offsets, n, ctx->cfg.k);
+    uint64_t cap = 1024;
+    while (cap < 2 * W) cap <<= 1;
+    DevBuf set, hist, ovf;
+    const uint32_t dense = ctx->g.bits == 8 ? 256u : 65536u;
+    SCB_TRY(set.ensure(cap * 8));
+    SCB_TRY(hist.ensure((uint64_t)dense * 8));
+    const uint64_t ovf_cap = ctx->g.bits == 32 ? std::max<uint64_t>(W, 1) : 1;
+    SCB_TRY(ovf.ensure(ovf_cap * 8));
+    SCB_CUDA(cudaMemset(set.p, 0xFF, cap * 8));
+    SCB_CUDA(cudaMemset(hist.p, 0, (uint64_t)dense * 8));
+    // the chunks run on the lane's non-blocking stream: finish the clears first
+    SCB_CUDA(cudaDeviceSynchronize());
+    uint64_t distinct = 0, queried = 0, n_ovf = 0;
+    SCB_TRY(for_each_chunk(ctx, seqs, offsets, n, [&](Lane& L, TileArgs& a, const Chunk&) -> scb_status {
+        a.set_keys = set.as<unsigned long long>();
+        a.set_mask = cap - 1;
+        a.hist = hist.as<unsigned long long>();
+        a.hist_dense = dense;
+        a.ovf = ovf.as<unsigned long long>() + n_ovf;
+        a.ovf_cap = ovf_cap - n_ovf;
+        SCB_TRY(query_device_batch(ctx, L, kModeDistinct, a, L.stream));
+        unsigned long long c[kCntSlots];
+        SCB_TRY(read_counters(ctx, L, L.stream, c));
+        distinct += c[kCntDistinct];
+        queried += c[kCntValid];
+        n_ovf += c[kCntOverflow];
+        return SCB_OK;
+    }));
+    std::vector<unsigned long long> h(dense), o(n_ovf);
+    SCB_CUDA(cudaMemcpy(h.data(), hist.p, (uint64_t)dense * 8, cudaMemcpyDeviceToHost));
+    if (n_ovf) SCB_CUDA(cudaMemcpy(o.data(), ovf.p, n_ovf * 8, cudaMemcpyDeviceToHost));
+    std::vector<std::pair<uint64_t, uint64_t>> rows;
+    rows_from_hist(h, o, rows);
+    if (distinct_keys) *distinct_keys = distinct;
+    if (queried_kmers) *queried_kmers = queried;
+    return emit_rows(rows, values, counts, capacity, n_rows);
+}
+
+scb_status scb_counter_histogram(scb_ctx* ctx, uint64_t* values, uint64_t* counts, uint64_t capacity,
+                                 uint64_t* n_rows) {
+    if (!ctx) return fail_kind(SCB_ERR_INTERNAL_STATE, "null context");
+    CtxLock lk(ctx);
+    const uint64_t slots = 1ull << ctx->cfg.counter_slots_exponent;
+    const uint32_t dense = ctx->g.bits == 8 ? 256u : 65536u;
+    const uint64_t ovf_cap = ctx->g.bits == 32 ? std::min<uint64_t>(slots, 1ull << 26) : 1;
+    DevBuf hist, ovf, cnt;
+    SCB_TRY(hist.ensure((uint64_t)dense * 8));
+    SCB_TRY(ovf.ensure(ovf_cap * 8));
+    SCB_TRY(cnt.ensure(8));
+    SCB_CUDA(cudaMemset(hist.p, 0, (uint64_t)dense * 8));
+    SCB_CUDA(cudaMemset(cnt.p, 0, 8));
+    launch_counter_hist(ctx->table, slots, ctx->g.bits, hist.as<unsigned long long>(), dense,
+                        ovf.as<unsigned long long>(), ovf_cap, cnt.as<unsigned long long>(), 0);
+    SCB_CUDA(cudaGetLastError());
+    unsigned long long n_ovf = 0;
+    SCB_CUDA(cudaMemcpy(&n_ovf, cnt.p, 8, cudaMemcpyDeviceToHost));
+    std::vector<unsigned long long> h(dense);
+    SCB_CUDA(cudaMemcpy(h.data(), hist.p, (uint64_t)dense * 8, cudaMemcpyDeviceToHost));
+    std::vector<std::pair<uint64_t, uint64_t>> rows;
+    if (n_ovf <= ovf_cap) {
+        std::vector<unsigned long long> o(n_ovf);
+        if (n_ovf) SCB_CUDA(cudaMemcpy(o.data(), ovf.p, n_ovf * 8, cudaMemcpyDeviceToHost));
+        rows_from_hist(h, std::move(o), rows);
+    } else {
+        // more large counters than the overflow list holds: histogram the table on the host
+        std::vector<uint32_t> t(slots);
+        SCB_CUDA(cudaMemcpy(t.data(), ctx->table, slots * 4, cudaMemcpyDeviceToHost));
+        std::sort(t.begin(), t.end());
+        for (size_t i = 0; i < t.size();) {
+            size_t j = i;
+            while (j < t.size() && t[j] == t[i]) j++;
+            rows.emplace_back(t[i], j - i);
+            i = j;
+        }
+    }
+    return emit_rows(rows, values, counts, capacity, n_rows);
+}
+
+scb_status scb_batch_stats(scb_ctx* ctx, const uint8_t* seqs, const uint64_t* offsets, uint64_t n,
+                           scb_stats* stats) {
+    if (!ctx || !stats) return fail_kind(SCB_ERR_INTERNAL_STATE, "null argument");
+    CtxLock lk(ctx);
+    std::memset(stats, 0, sizeof(*stats));
+    return for_each_chunk(ctx, seqs, offsets, n, [&](Lane& L, TileArgs& a, const Chunk&) -> scb_status {
+        SCB_TRY(run_tiles(ctx, L, kModeStats, a, L.stream));
+        unsigned long long c[kCntSlots];
+        SCB_TRY(read_counters(ctx, L, L.stream, c));
+        stats->windows += c[kCntWindows];
+        stats->super_kmers += c[kCntSuperKmers];
+        stats->smers += c[kCntSmers];
+        stats->sectors += c[kCntSectors];
+        return SCB_OK;
+    });
+}
+
+scb_status scb_debug_window_minimizers(scb_ctx* ctx, const uint8_t* seqs, const uint64_t* offsets, uint64_t n,
+                                       uint32_t* out) {
+    if (!ctx || !out) return fail_kind(SCB_ERR_INTERNAL_STATE, "null argument");
+    CtxLock lk(ctx);
+    DevBuf dbg;
+    return for_each_chunk(ctx, seqs, offsets, n, [&](Lane& L, TileArgs& a, const Chunk& ch) -> scb_status {
+        const uint64_t nb = ch.byte1 - ch.byte0;
+        SCB_TRY(dbg.ensure(std::max<uint64_t>(nb, 1) * 4));
+        launch_fill_u32(dbg.as<uint32_t>(), 0xFFFFFFFFu, nb, L.stream);
+        a.dbg = dbg.as<uint32_t>();
+        SCB_TRY(run_tiles(ctx, L, kModeDebugMin, a, L.stream));
+        unsigned long long c[kCntSlots];
+        SCB_TRY(read_counters(ctx, L, L.stream, c));
+        std::vector<uint32_t> h(nb);
+        if (nb) SCB_CUDA(cudaMemcpy(h.data(), dbg.p, nb * 4, cudaMemcpyDeviceToHost));
+        for (uint64_t i = 0; i < nb; i++) {
+            out[ch.byte0 - offsets[0] + i] = h[i] == 0xFFFFFFFFu ? h[i] : (uint32_t)(h[i] + ch.byte0 - offsets[0]);
+        }
+        return SCB_OK;
+    });
+}
+
+scb_status scb_set_timing(scb_ctx* ctx, int enable) {
+    if (!ctx) return fail_kind(SCB_ERR_INTERNAL_STATE, "null context");
+    CtxLock lk(ctx);
+    if (enable) {
+        for (auto& e : ctx->lane.ev) {
+            if (!e) SCB_CUDA(cudaEventCreate(&e));
+        }
+    }
+    ctx->timing = enable != 0;
+    ctx->times = scb_timings{};
+    ctx->lane.pack_timed = false;
+    ctx->lane.main_kind = 0;
+    return SCB_OK;
+}
+
+scb_status scb_get_timings(const scb_ctx* ctx, scb_timings* out) {
+    if (!ctx || !out) return fail_kind(SCB_ERR_INTERNAL_STATE, "null argument");
+    *out = ctx->times;
+    return SCB_OK;
+}
+
+scb_status scb_reset(scb_ctx* ctx) {
+    if (!ctx) return fail_kind(SCB_ERR_INTERNAL_STATE, "null context");
+    CtxLock lk(ctx);
+    SCB_CUDA(cudaMemset(ctx->table, 0, ctx->table_bytes));
+    SCB_CUDA(cudaMemset(ctx->status, 0, 64));
+    SCB_CUDA(cudaDeviceSynchronize());
+    ctx->inserted_kmers = 0;
+    ctx->inserted_smers = 0;
+    ctx->frozen = false;
+    return SCB_OK;
+}
+
+uint64_t scb_table_bytes(const scb_ctx* ctx) { return ctx ? ctx->table_bytes : 0; }
+
+scb_status scb_table_download(const scb_ctx* cctx, void* host, uint64_t bytes) {
+    if (!cctx || !host) return fail_kind(SCB_ERR_INTERNAL_STATE, "null argument");
+    scb_ctx* ctx = const_cast<scb_ctx*>(cctx);
+    CtxLock lk(ctx);
+    if (bytes != ctx->table_bytes) return fail_kind(SCB_ERR_INTERNAL_STATE, "table size mismatch");
+    SCB_CUDA(cudaMemcpy(host, ctx->table, bytes, cudaMemcpyDeviceToHost));
+    return SCB_OK;
+}
+
+scb_status scb_table_upload(scb_ctx* ctx, const void* host, uint64_t bytes, uint64_t inserted_kmers) {
+    if (!ctx || !host) return fail_kind(SCB_ERR_INTERNAL_STATE, "null argument");
+    CtxLock lk(ctx);
+    if (bytes != ctx->table_bytes) return fail_kind(SCB_ERR_INTERNAL_STATE, "table size mismatch");
+    SCB_CUDA(cudaMemcpy(ctx->table, host, bytes, cudaMemcpyHostToDevice));
+    ctx->inserted_kmers = inserted_kmers;
+    ctx->frozen = true;
+    return SCB_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// .scb (api.rs:28-29, 388-608)
+// ---------------------------------------------------------------------------------------
+static void put64(std::vector<uint8_t>& b, uint64_t v) {
+    for (int i = 0; i < 8; i++) b.push_back((uint8_t)(v >> (8 * i)));
+}
+static void put32(std::vector<uint8_t>& b, uint32_t v) {
+    for (int i = 0; i < 4; i++) b.push_back((uint8_t)(v >> (8 * i)));
+}
+
+static const uint8_t kMagic[8] = {'S', 'C', 'B', 'I', 'D', 'X', 0, 0};
+static const uint32_t kFormatVersion = 2;
+
+scb_status scb_save(const scb_ctx* cctx, const char* path) {
+    if (!cctx || !path) return fail_kind(SCB_ERR_INTERNAL_STATE, "null argument");
+    scb_ctx* ctx = const_cast<scb_ctx*>(cctx);
+    CtxLock lk(ctx);
+    std::vector<uint8_t> head;
+    head.insert(head.end(), kMagic, kMagic + 8);
+    put32(head, kFormatVersion);
+    const scb_config& c = ctx->cfg;
+    put64(head, c.k);
+    put64(head, c.m);
+    put64(head, c.s);
+    put64(head, c.n_hashes);
+    head.push_back(c.counter_bits);
+    head.push_back(c.counter_slots_exponent);
+    head.push_back(c.block_slots_exponent);
+    put64(head, c.threads);
+    put64(head, c.queue);
+    put64(head, ctx->inserted_kmers);
+    put64(head, ctx->shard_count);
+    put64(head, ctx->subblocks);
+    put64(head, ctx->block_slots);
+    put64(head, ctx->shard_mask);
+    put32(head, ctx->shard_shift);
+    put64(head, ctx->block_slots_mask);
+    put64(head, ctx->nb_blocks);
+    put64(head, ctx->block_mask);
+    put64(head, c.n_hashes);
+    FILE* fp = std::fopen(path, "wb");
+    if (!fp) return fail(SCB_ERR_IO, std::string("I/O error for '") + path + "': cannot create file");
+    bool ok = std::fwrite(head.data(), 1, head.size(), fp) == head.size();
+    // the table is already in file order: stream it through a pinned buffer
+    const uint64_t chunk = 64ull << 20;
+    void* pinned = nullptr;
+    if (cudaMallocHost(&pinned, chunk) != cudaSuccess) {
+        std::fclose(fp);
+        return fail_kind(SCB_ERR_INTERNAL_STATE, "pinned host allocation failed");
+    }
+    for (uint64_t off = 0; ok && off < ctx->table_bytes; off += chunk) {
+        const uint64_t nb = std::min(chunk, ctx->table_bytes - off);
+        if (cudaMemcpy(pinned, (const uint8_t*)ctx->table + off, nb, cudaMemcpyDeviceToHost) != cudaSuccess) {
+            ok = false;
+            break;
+        }
+        ok = std::fwrite(pinned, 1, nb, fp) == nb;
+    }
+    cudaFreeHost(pinned);
+    ok = (std::fclose(fp) == 0) && ok;
+    if (!ok) return fail(SCB_ERR_IO, std::string("I/O error for '") + path + "': write failed");
+    return SCB_OK;
+}
+
+static bool get_exact(FILE* fp, void* dst, size_t n) { return std::fread(dst, 1, n, fp) == n; }
+static bool get64(FILE* fp, uint64_t& v) {
+    uint8_t b[8];
+    if (!get_exact(fp, b, 8)) return false;
+    v = 0;
+    for (int i = 0; i < 8; i++) v |= (uint64_t)b[i] << (8 * i);
+    return true;
+}
+static bool get32(FILE* fp, uint32_t& v) {
+    uint8_t b[4];
+    if (!get_exact(fp, b, 4)) return false;
+    v = 0;
+    for (int i = 0; i < 4; i++) v |= (uint32_t)b[i] << (8 * i);
+    return true;
+}
+
+scb_status scb_load(const char* path, scb_ctx** out) {
+    if (!path || !out) return fail_kind(SCB_ERR_INTERNAL_STATE, "null argument");
+    *out = nullptr;
+    FILE* fp = std::fopen(path, "rb");
+    if (!fp) return fail(SCB_ERR_IO, std::string("I/O error for '") + path + "': cannot open file");
+    struct Closer {
+        FILE* f;
+        ~Closer() { std::fclose(f); }
+    } closer{fp};
+    const std::string io_short = std::string("I/O error for '") + path + "': failed to fill whole buffer";
+    uint8_t magic[8];
+    if (!get_exact(fp, magic, 8)) return fail(SCB_ERR_IO, io_short);
+    if (std::memcmp(magic, kMagic, 8) != 0)
+        return fail_kind(SCB_ERR_INVALID_INDEX_FORMAT, "bad SuperCountingBloom index magic");
+    uint32_t version = 0;
+    if (!get32(fp, version)) return fail(SCB_ERR_IO, io_short);
+    if (version != kFormatVersion)
+        return fail_kind(SCB_ERR_INVALID_INDEX_FORMAT, "unsupported index format version " + std::to_string(version));
+    scb_config c{};
+    if (!get64(fp, c.k) || !get64(fp, c.m) || !get64(fp, c.s) || !get64(fp, c.n_hashes) ||
+        !get_exact(fp, &c.counter_bits, 1))
+        return fail(SCB_ERR_IO, io_short);
+    if (c.counter_bits != 8 && c.counter_bits != 16 && c.counter_bits != 32)
+        return fail_kind(SCB_ERR_INVALID_INDEX_FORMAT, "unsupported counter width " + std::to_string(c.counter_bits));
+    uint64_t inserted = 0;
+    if (!get_exact(fp, &c.counter_slots_exponent, 1) || !get_exact(fp, &c.block_slots_exponent, 1) ||
+        !get64(fp, c.threads) || !get64(fp, c.queue) || !get64(fp, inserted))
+        return fail(SCB_ERR_IO, io_short);
+    SCB_TRY(validate_config(&c));
+    uint64_t sc, sb, bs, sm, bsm, nb, bm, nh;
+    uint32_t ss;
+    if (!get64(fp, sc) || !get64(fp, sb) || !get64(fp, bs) || !get64(fp, sm) || !get32(fp, ss) || !get64(fp, bsm) ||
+        !get64(fp, nb) || !get64(fp, bm) || !get64(fp, nh))
+        return fail(SCB_ERR_IO, io_short);
+    scb_ctx probe;
+    probe.cfg = c;
+    fill_geometry(&probe);
+    if (sc != probe.shard_count || sb != probe.subblocks || bs != probe.block_slots || sm != probe.shard_mask ||
+        ss != probe.shard_shift || bsm != probe.block_slots_mask || nb != probe.nb_blocks || bm != probe.block_mask ||
+        nh != c.n_hashes)
+        return fail_kind(SCB_ERR_INVALID_INDEX_FORMAT, "stored filter layout does not match config");
+    scb_ctx* ctx = nullptr;
+    SCB_TRY(alloc_ctx(&c, &ctx));
+    const uint64_t chunk = 64ull << 20;
+    void* pinned = nullptr;
+    if (cudaMallocHost(&pinned, chunk) != cudaSuccess) {
+        delete ctx;
+        return fail_kind(SCB_ERR_INTERNAL_STATE, "pinned host allocation failed");
+    }
+    for (uint64_t off = 0; off < ctx->table_bytes; off += chunk) {
+        const uint64_t nbytes = std::min(chunk, ctx->table_bytes - off);
+        if (!get_exact(fp, pinned, nbytes)) {
+            cudaFreeHost(pinned);
+            delete ctx;
+            return fail(SCB_ERR_IO, io_short);
+        }
+        if (cudaMemcpy((uint8_t*)ctx->table + off, pinned, nbytes, cudaMemcpyHostToDevice) != cudaSuccess) {
+            cudaFreeHost(pinned);
+            delete ctx;
+            return fail_kind(SCB_ERR_INTERNAL_STATE, "table upload failed");
+        }
+    }
+    cudaFreeHost(pinned);
+    uint8_t extra;
+    if (std::fread(&extra, 1, 1, fp) == 1) {
+        delete ctx;
+        return fail_kind(SCB_ERR_INVALID_INDEX_FORMAT, "trailing bytes after serialized index");
+    }
+    ctx->inserted_kmers = inserted;
+    ctx->frozen = true;
+    *out = ctx;
+    return SCB_OK;
+}
+
+}  // extern "C"

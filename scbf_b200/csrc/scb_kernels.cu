@@ -1,0 +1,683 @@
+// SuperCountingBloom kernels for sm_100a.
+//
+//  (a) k_pack          ASCII -> 2-bit codes + ACGT bitmap, 32 bytes per thread, vector loads
+//  (b)-(f) k_tiles     one persistent kernel over a device work queue of 1024-window tiles of
+//                      the flat base stream.  A tile stages its codes and bitmaps in shared
+//                      memory, computes the canonical m-mer hash keys once, picks each window's
+//                      minimizer (kernel b), hashes s-mers (c) and then inserts (d), queries
+//                      (e) or feeds the distinct-k-mer spectrum (f).  Reads of any length share
+//                      the same tiles, so 150 bp and 100 kbp reads balance without per-read work.
+//  plain pipeline      k_tiles<Materialize> writes per-window block ids and super-k-mer end
+//                      flags to HBM, then k_plain_insert / k_plain_query run one thread per
+//                      window from global memory: the one-launch-per-stage baseline.
+//
+// Insert semantics (filter.rs:199-237) in per-window form: super-k-mer j with windows
+// [a_j, e_j] inserts s-mers a_j .. e_j + k - s into its block.  Window g therefore inserts its
+// own s-mer g, and the last window of each super-k-mer also inserts s-mers g+1 .. g+k-s.
+// Saturating increments commute, so any order gives the reference's counters.
+// Query semantics (filter.rs:462-508): window g's estimate is the min over s-mers g .. g+k-s of
+// their n_hashes-probe minimum inside window g's block, which is what the reference's deque
+// computes per super-k-mer.
+#include <atomic>
+#include <cstdio>
+
+#include "scb_kernels.cuh"
+
+namespace scb {
+
+namespace {
+std::atomic<uint64_t> g_launches{0};
+}
+
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+uint64_t kernel_launch_count() { return g_launches.load(std::memory_order_relaxed); }
+
+// ---------------------------------------------------------------------------------------
+// (a) packing
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ void pack_word(uint32_t w, uint32_t& code8, uint32_t& valid4) {
+    const uint32_t u = w & 0xDFDFDFDFu;  // upper-case letters
+    const uint32_t m = __vcmpeq4(u, 0x41414141u) | __vcmpeq4(u, 0x43434343u) | __vcmpeq4(u, 0x47474747u) |
+                       __vcmpeq4(u, 0x54545454u);
+    uint32_t c = (w >> 1) & 0x03030303u;
+    code8 = (c | (c >> 6) | (c >> 12) | (c >> 18)) & 0xFFu;
+    uint32_t v = m & 0x01010101u;
+    valid4 = (v | (v >> 7) | (v >> 14) | (v >> 21)) & 0xFu;
+}
+
+__global__ void k_pack(const uint8_t* __restrict__ ascii, uint64_t n, uint32_t* __restrict__ codes,
+                       uint32_t* __restrict__ valid, uint64_t n_groups, int aligned) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t gi = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; gi < n_groups; gi += stride) {
+        const uint64_t base = gi * 32;
+        uint32_t w[8];
+        if (aligned && base + 32 <= n) {
+            const uint4 x = __ldcs(reinterpret_cast<const uint4*>(ascii + base));
+            const uint4 y = __ldcs(reinterpret_cast<const uint4*>(ascii + base + 16));
+            w[0] = x.x; w[1] = x.y; w[2] = x.z; w[3] = x.w;
+            w[4] = y.x; w[5] = y.y; w[6] = y.z; w[7] = y.w;
+        } else {
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                uint32_t v = 0;
+                for (int b = 0; b < 4; b++) {
+                    const uint64_t idx = base + 4 * j + b;
+                    if (idx < n) v |= (uint32_t)ascii[idx] << (8 * b);
+                }
+                w[j] = v;
+            }
+        }
+        uint32_t c0 = 0, c1 = 0, vm = 0;
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            uint32_t c8, v4;
+            pack_word(w[j], c8, v4);
+            if (j < 4) {
+                c0 |= c8 << (8 * j);
+            } else {
+                c1 |= c8 << (8 * (j - 4));
+            }
+            vm |= v4 << (4 * j);
+        }
+        codes[2 * gi] = c0;
+        codes[2 * gi + 1] = c1;
+        valid[gi] = vm;
+    }
+}
+
+__global__ void k_seqstart(const uint64_t* __restrict__ offsets, uint64_t n_seqs, uint64_t n_bytes,
+                           uint32_t* __restrict__ seqstart) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n_seqs; j += stride) {
+        const uint64_t a = offsets[j], b = offsets[j + 1];
+        if (b > a && a < n_bytes) atomicOr(&seqstart[a >> 5], 1u << (a & 31));
+    }
+}
+
+// Per-sequence window counts: woff[j] = max(0, len_j + 1 - k) (scanned afterwards), plus the
+// records / total-windows fields of the report (api.rs:284-285).
+__global__ void k_seq_windows(const uint64_t* __restrict__ offsets, uint64_t n_seqs, uint32_t k,
+                              unsigned long long* cnt, uint64_t* woff) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    unsigned long long total = 0, recs = 0;
+    const uint64_t n_iter = (n_seqs + stride - 1) / stride;
+    for (uint64_t it = 0; it < n_iter; it++) {
+        const uint64_t j = it * stride + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+        if (j < n_seqs) {
+            const uint64_t len = offsets[j + 1] - offsets[j];
+            const uint64_t nw = len >= k ? len + 1 - k : 0;
+            if (woff) woff[j] = nw;
+            total += nw;
+            recs += 1;
+        }
+    }
+    warp_add_u64(&cnt[kCntTotalWindows], total);
+    warp_add_u64(&cnt[kCntRecords], recs);
+}
+
+// Exclusive scan of u64 (three phases, recursive over block sums).
+constexpr int kScanThreads = 1024;
+
+__global__ void k_scan_blocks(uint64_t* data, uint64_t n, uint64_t* block_sums) {
+    __shared__ uint64_t warp_tot[32];
+    const uint64_t i = (uint64_t)blockIdx.x * kScanThreads + threadIdx.x;
+    const uint64_t v = i < n ? data[i] : 0;
+    uint64_t x = v;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int off = 1; off < 32; off <<= 1) {
+        const uint64_t y = __shfl_up_sync(0xFFFFFFFFu, x, off);
+        if (lane >= off) x += y;
+    }
+    if (lane == 31) warp_tot[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        uint64_t t = warp_tot[lane];
+        for (int off = 1; off < 32; off <<= 1) {
+            const uint64_t y = __shfl_up_sync(0xFFFFFFFFu, t, off);
+            if (lane >= off) t += y;
+        }
+        warp_tot[lane] = t;
+    }
+    __syncthreads();
+    const uint64_t incl = x + (wid > 0 ? warp_tot[wid - 1] : 0);
+    if (i < n) data[i] = incl - v;
+    if (threadIdx.x == kScanThreads - 1) block_sums[blockIdx.x] = incl;
+}
+
+__global__ void k_scan_add(uint64_t* data, uint64_t n, const uint64_t* block_prefix) {
+    const uint64_t i = (uint64_t)blockIdx.x * kScanThreads + threadIdx.x;
+    if (i < n) data[i] += block_prefix[blockIdx.x];
+}
+
+void launch_scan_inplace(uint64_t* data, uint64_t n, uint64_t* scratch, cudaStream_t st) {
+    if (n == 0) return;
+    const uint64_t nb = (n + kScanThreads - 1) / kScanThreads;
+    k_scan_blocks<<<(unsigned)nb, kScanThreads, 0, st>>>(data, n, scratch);
+    note_launch();
+    if (nb > 1) {
+        launch_scan_inplace(scratch, nb, scratch + nb, st);
+        k_scan_add<<<(unsigned)nb, kScanThreads, 0, st>>>(data, n, scratch);
+        note_launch();
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Tile kernel
+// ---------------------------------------------------------------------------------------
+constexpr int kBack = 32;  // windows evaluated before a tile in stats mode (>= w)
+constexpr int kFwd = 1;    // windows evaluated after a tile (super-k-mer end detection)
+constexpr int kEvalMax = kTileWindows + kBack + kFwd;
+constexpr int kKeysMax = kEvalMax + 32;
+constexpr int kCodeWordsMax = (kEvalMax + 96 + 16) / 16 + 8;
+constexpr int kBitWordsMax = (kEvalMax + 128 + 32) / 32 + 8;
+constexpr uint16_t kNoWindow = 0xFFFFu;
+
+struct TileSmem {
+    uint32_t codes[kCodeWordsMax];
+    uint32_t valid[kBitWordsMax];
+    uint32_t start[kBitWordsMax];
+    uint16_t key[kKeysMax];
+    uint16_t poff[kEvalMax];
+    uint32_t block[kEvalMax];
+    uint16_t ends[kTileWindows];
+    uint32_t n_ends;
+    uint32_t tile;
+    uint64_t seq_lo, seq_hi;
+};
+
+__device__ __forceinline__ uint32_t code_at(const uint32_t* words, uint64_t b) {
+    return (words[b >> 4] >> (2 * (b & 15))) & 3u;
+}
+
+// Largest j in [lo, hi] with offsets[j] <= pos.
+__device__ __forceinline__ uint64_t seq_of(const uint64_t* offsets, uint64_t lo, uint64_t hi, uint64_t pos) {
+    while (lo < hi) {
+        const uint64_t mid = (lo + hi + 1) >> 1;
+        if (__ldg(offsets + mid) <= pos) {
+            lo = mid;
+        } else {
+            hi = mid - 1;
+        }
+    }
+    return lo;
+}
+
+__device__ __forceinline__ bool set_insert(unsigned long long* keys, uint64_t mask, uint64_t key, uint32_t* status) {
+    uint64_t i = xorshift64(key ^ 0x5851F42D4C957F2Dull) & mask;
+    for (uint64_t probe = 0; probe <= mask; probe++) {
+        const unsigned long long cur = __ldcg(keys + i);
+        if (cur == key) return false;
+        if (cur == ~0ull) {
+            const unsigned long long prev = atomicCAS(keys + i, ~0ull, (unsigned long long)key);
+            if (prev == ~0ull) return true;
+            if (prev == key) return false;
+        }
+        i = (i + 1) & mask;
+    }
+    atomicOr(status, kStatusHashFull);
+    return false;
+}
+
+template <int BITS>
+__device__ __forceinline__ uint32_t window_estimate(const TileArgs& a, const DevGeom& g, const uint32_t* codes_s,
+                                                    uint64_t rel, uint64_t base) {
+    uint32_t r = CounterTraits<BITS>::kMax;
+    const uint64_t sm = len_mask(g.s);
+    for (uint32_t t = 0; t + g.s <= g.k; t++) {
+        const uint64_t smer = canonical(codes64(codes_s, rel + t) & sm, g.s);
+        const uint32_t e = estimate_smer<BITS>(a.table, g, base, smer);
+        r = e < r ? e : r;
+    }
+    return r;
+}
+
+template <int MODE, int BITS>
+__global__ void __launch_bounds__(kTileThreads) k_tiles(TileArgs a) {
+    __shared__ TileSmem sm;
+    const DevGeom g = a.g;
+    const uint32_t tid = threadIdx.x;
+    uint32_t* table32 = reinterpret_cast<uint32_t*>(a.table);
+    unsigned long long c_win = 0, c_smer = 0, c_valid = 0, c_pos = 0, c_sum = 0, c_sk = 0, c_sec = 0, c_dist = 0;
+    const uint64_t s_mask = len_mask(g.s);
+    const uint32_t ks = g.k - g.s;
+
+    while (true) {
+        if (tid == 0) sm.tile = atomicAdd(a.tile_counter, 1u);
+        __syncthreads();
+        const uint32_t tile = sm.tile;
+        if (tile >= a.n_tiles) break;
+        const uint64_t t0 = (uint64_t)tile * kTileWindows;
+        const uint32_t back = (MODE == kModeStats) ? (uint32_t)(t0 < (uint64_t)kBack ? t0 : (uint64_t)kBack) : 0u;
+        const uint64_t e0 = t0 - back;
+        const uint32_t n_eval = back + kTileWindows + kFwd;
+        const uint32_t n_keys = n_eval + g.w - 1;
+
+        // stage codes and bitmaps of the tile
+        const uint64_t cb = e0 & ~15ull;
+        const uint64_t cw0 = cb >> 4;
+        const uint32_t n_cw = (uint32_t)((e0 + n_eval + 96 - cb) >> 4) + 3;
+        for (uint32_t i = tid; i < n_cw; i += blockDim.x) {
+            sm.codes[i] = (cw0 + i < a.n_code_words) ? __ldg(a.codes + cw0 + i) : 0u;
+        }
+        const uint64_t bb = e0 & ~31ull;
+        const uint64_t bw0 = bb >> 5;
+        const uint32_t n_bw = (uint32_t)((e0 + n_eval + 128 - bb) >> 5) + 3;
+        for (uint32_t i = tid; i < n_bw; i += blockDim.x) {
+            const bool in = bw0 + i < a.n_bit_words;
+            sm.valid[i] = in ? __ldg(a.valid + bw0 + i) : 0u;
+            sm.start[i] = in ? __ldg(a.seqstart + bw0 + i) : 0u;
+        }
+        if (MODE == kModeAbund && tid == 0) {
+            sm.seq_lo = seq_of(a.offsets, 0, a.n_seqs, t0);
+            const uint64_t last = t0 + kTileWindows;
+            sm.seq_hi = seq_of(a.offsets, sm.seq_lo, a.n_seqs, last);
+        }
+        if (tid == 0) sm.n_ends = 0;
+        __syncthreads();
+
+        // canonical m-mer hash keys (upper 16 bits) for m-mer positions e0 .. e0 + n_keys - 1
+        {
+            const uint32_t per = (n_keys + blockDim.x - 1) / blockDim.x;
+            const uint32_t q0 = tid * per;
+            const uint32_t q1 = min(q0 + per, n_keys);
+            if (q0 < q1) {
+                const uint64_t b0 = e0 + q0 - cb;
+                uint32_t fw, rc;
+                nt_direct(codes64(sm.codes, b0) & len_mask(g.m), g.m, fw, rc);
+                sm.key[q0] = (uint16_t)((fw + rc) >> 16);
+                for (uint32_t q = q0 + 1; q < q1; q++) {
+                    const uint64_t b = e0 + q - cb;
+                    nt_roll(fw, rc, code_at(sm.codes, b - 1), code_at(sm.codes, b + g.m - 1), g.m);
+                    sm.key[q] = (uint16_t)((fw + rc) >> 16);
+                }
+            }
+        }
+        __syncthreads();
+
+        // (b) minimizer of each evaluated window and its block
+        for (uint32_t i = tid; i < n_eval; i += blockDim.x) {
+            const uint64_t pos = e0 + i;
+            uint16_t po = kNoWindow;
+            if (window_ok(bits64(sm.valid, pos - bb), bits64(sm.start, pos - bb), g.k)) {
+                uint32_t best = 0xFFFFFFFFu, left = 0, right = 0;
+                for (uint32_t o = 0; o < g.w; o++) {
+                    const uint32_t key = sm.key[i + o];
+                    if (key < best) {
+                        best = key;
+                        left = right = o;
+                    } else if (key == best) {
+                        right = o;
+                    }
+                }
+                const uint64_t kv = codes64(sm.codes, pos - cb) & len_mask(g.k);
+                const uint32_t tg = __popcll(kv & 0xAAAAAAAAAAAAAAAAull);
+                po = (uint16_t)(i + ((2 * tg > g.k) ? left : right));
+                const uint64_t mm = codes64(sm.codes, e0 + po - cb) & len_mask(g.m);
+                sm.block[i] = (uint32_t)(xorshift64(canonical(mm, g.m)) & g.block_mask);
+            }
+            sm.poff[i] = po;
+        }
+        __syncthreads();
+
+        if constexpr (MODE == kModeInsert) {
+            for (uint32_t i = tid; i < kTileWindows; i += blockDim.x) {
+                const uint16_t po = sm.poff[i];
+                if (po == kNoWindow) continue;
+                const uint64_t pos = t0 + i;
+                const uint64_t base = block_base(g, sm.block[i]);
+                const uint64_t smer = canonical(codes64(sm.codes, pos - cb) & s_mask, g.s);
+                insert_smer<BITS>(table32, g, base, smer, a.status);
+                c_win++;
+                c_smer++;
+                if (sm.poff[i + 1] != po) {
+                    c_sk++;
+                    if (ks > 0) sm.ends[atomicAdd(&sm.n_ends, 1u)] = (uint16_t)i;
+                }
+            }
+            __syncthreads();
+            const uint32_t n_tasks = sm.n_ends * ks;
+            for (uint32_t f = tid; f < n_tasks; f += blockDim.x) {
+                const uint32_t e = sm.ends[f / ks];
+                const uint32_t u = 1 + f % ks;
+                const uint64_t smer = canonical(codes64(sm.codes, t0 + e + u - cb) & s_mask, g.s);
+                insert_smer<BITS>(table32, g, block_base(g, sm.block[e]), smer, a.status);
+                c_smer++;
+            }
+        } else if constexpr (MODE == kModeReport || MODE == kModeAbund || MODE == kModeDistinct) {
+            for (uint32_t i = tid; i < kTileWindows; i += blockDim.x) {
+                if (sm.poff[i] == kNoWindow) continue;
+                const uint64_t pos = t0 + i;
+                const uint32_t r = window_estimate<BITS>(a, g, sm.codes, pos - cb, block_base(g, sm.block[i]));
+                if constexpr (MODE == kModeReport) {
+                    c_valid++;
+                    c_pos += r > 0;
+                    c_sum += r;
+                } else if constexpr (MODE == kModeAbund) {
+                    const uint64_t j = seq_of(a.offsets, sm.seq_lo, sm.seq_hi, pos);
+                    const uint64_t o = a.woff[j] + (pos - __ldg(a.offsets + j));
+                    a.out[o] = r;
+                    a.out_valid[o] = 1;
+                } else {
+                    c_valid++;
+                    const uint64_t key = canonical(codes64(sm.codes, pos - cb) & len_mask(g.k), g.k);
+                    if (set_insert(a.set_keys, a.set_mask, key, a.status)) {
+                        c_dist++;
+                        if (r < a.hist_dense) {
+                            atomicAdd(a.hist + r, 1ull);
+                        } else {
+                            const unsigned long long o = atomicAdd(&a.cnt[kCntOverflow], 1ull);
+                            if (o < a.ovf_cap) {
+                                a.ovf[o] = r;
+                            } else {
+                                atomicOr(a.status, kStatusOverflowFull);
+                            }
+                        }
+                    }
+                }
+            }
+        } else if constexpr (MODE == kModeStats) {
+            const uint32_t bytes_per = BITS / 8;
+            const uint64_t block_sectors = ((1ull << g.block_log2) * bytes_per + 31) / 32;
+            for (uint32_t i = back + tid; i < back + kTileWindows; i += blockDim.x) {
+                const uint16_t po = sm.poff[i];
+                if (po == kNoWindow) continue;
+                c_win++;
+                if (sm.poff[i + 1] == po) continue;
+                c_sk++;
+                uint32_t st = i;
+                while (st > 0 && sm.poff[st - 1] == po) st--;
+                const uint32_t n_sm = (i - st + 1) + ks;
+                c_smer += n_sm;
+                if (block_sectors <= 256) {
+                    uint32_t seen[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+                    const uint64_t base_rel = 0;
+                    (void)base_rel;
+                    for (uint32_t q = 0; q < n_sm; q++) {
+                        const uint64_t smer = canonical(codes64(sm.codes, e0 + st + q - cb) & s_mask, g.s);
+                        uint64_t hash = xorshift64(smer);
+                        for (uint32_t h = 0; h < g.h; h++) {
+                            const uint32_t sec = (uint32_t)(((hash & g.bs_mask) * bytes_per) >> 5);
+                            seen[sec >> 5] |= 1u << (sec & 31);
+                            hash = xorshift64(hash);
+                        }
+                    }
+                    uint32_t d = 0;
+                    for (int x = 0; x < 8; x++) d += __popc(seen[x]);
+                    c_sec += d;
+                } else {
+                    c_sec += (unsigned long long)n_sm * g.h;
+                }
+            }
+        } else if constexpr (MODE == kModeDebugMin) {
+            for (uint32_t i = tid; i < kTileWindows; i += blockDim.x) {
+                const uint64_t pos = t0 + i;
+                if (sm.poff[i] != kNoWindow && pos < a.n_bytes) a.dbg[pos] = (uint32_t)(e0 + sm.poff[i]);
+            }
+        } else if constexpr (MODE == kModeMaterialize) {
+            for (uint32_t i = tid; i < kTileWindows; i += blockDim.x) {
+                const uint64_t pos = t0 + i;
+                if (pos >= a.n_bytes) continue;
+                const uint16_t po = sm.poff[i];
+                a.wblock[pos] = po == kNoWindow ? 0xFFFFFFFFu : sm.block[i];
+                a.wend[pos] = (po != kNoWindow && sm.poff[i + 1] != po) ? 1 : 0;
+            }
+        }
+        __syncthreads();
+    }
+    warp_add_u64(&a.cnt[kCntWindows], c_win);
+    warp_add_u64(&a.cnt[kCntSmers], c_smer);
+    warp_add_u64(&a.cnt[kCntValid], c_valid);
+    warp_add_u64(&a.cnt[kCntPositive], c_pos);
+    warp_add_u64(&a.cnt[kCntChecksum], c_sum);
+    warp_add_u64(&a.cnt[kCntSuperKmers], c_sk);
+    warp_add_u64(&a.cnt[kCntSectors], c_sec);
+    warp_add_u64(&a.cnt[kCntDistinct], c_dist);
+}
+
+template <int MODE>
+static void launch_tiles_bits(const TileArgs& a, int grid, cudaStream_t st) {
+    switch (a.g.bits) {
+        case 8: k_tiles<MODE, 8><<<grid, kTileThreads, 0, st>>>(a); break;
+        case 16: k_tiles<MODE, 16><<<grid, kTileThreads, 0, st>>>(a); break;
+        default: k_tiles<MODE, 32><<<grid, kTileThreads, 0, st>>>(a); break;
+    }
+    note_launch();
+}
+
+void launch_tiles(int mode, const TileArgs& a, int grid, cudaStream_t st) {
+    if (grid <= 0) return;
+    switch (mode) {
+        case kModeInsert: launch_tiles_bits<kModeInsert>(a, grid, st); break;
+        case kModeReport: launch_tiles_bits<kModeReport>(a, grid, st); break;
+        case kModeAbund: launch_tiles_bits<kModeAbund>(a, grid, st); break;
+        case kModeDistinct: launch_tiles_bits<kModeDistinct>(a, grid, st); break;
+        case kModeStats: launch_tiles_bits<kModeStats>(a, grid, st); break;
+        case kModeDebugMin: launch_tiles_bits<kModeDebugMin>(a, grid, st); break;
+        case kModeMaterialize: launch_tiles_bits<kModeMaterialize>(a, grid, st); break;
+        default: break;
+    }
+}
+
+int tile_grid(int mode, int bits, int sm_count, uint32_t n_tiles) {
+    int per_sm = 0;
+    const void* fn = nullptr;
+#define SCB_PICK(MODEV)                                                              \
+    fn = bits == 8 ? (const void*)k_tiles<MODEV, 8>                                  \
+                   : (bits == 16 ? (const void*)k_tiles<MODEV, 16> : (const void*)k_tiles<MODEV, 32>)
+    switch (mode) {
+        case kModeInsert: SCB_PICK(kModeInsert); break;
+        case kModeReport: SCB_PICK(kModeReport); break;
+        case kModeAbund: SCB_PICK(kModeAbund); break;
+        case kModeDistinct: SCB_PICK(kModeDistinct); break;
+        case kModeStats: SCB_PICK(kModeStats); break;
+        case kModeDebugMin: SCB_PICK(kModeDebugMin); break;
+        default: SCB_PICK(kModeMaterialize); break;
+    }
+#undef SCB_PICK
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kTileThreads, 0) != cudaSuccess || per_sm < 1) {
+        per_sm = 1;
+    }
+    const uint64_t want = (uint64_t)per_sm * (uint64_t)sm_count;
+    return (int)(n_tiles < want ? n_tiles : want);
+}
+
+// ---------------------------------------------------------------------------------------
+// Plain pipeline: one thread per window, everything from global memory.
+// ---------------------------------------------------------------------------------------
+template <int BITS>
+__global__ void k_plain_insert(TileArgs a) {
+    const DevGeom g = a.g;
+    uint32_t* table32 = reinterpret_cast<uint32_t*>(a.table);
+    const uint64_t s_mask = len_mask(g.s);
+    const uint32_t ks = g.k - g.s;
+    unsigned long long c_win = 0, c_smer = 0, c_sk = 0;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t n_iter = (a.n_bytes + stride - 1) / stride;
+    for (uint64_t it = 0; it < n_iter; it++) {
+        const uint64_t pos = it * stride + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+        if (pos >= a.n_bytes) continue;
+        const uint32_t blk = a.wblock[pos];
+        if (blk == 0xFFFFFFFFu) continue;
+        const uint64_t base = block_base(g, blk);
+        insert_smer<BITS>(table32, g, base, canonical(codes64(a.codes, pos) & s_mask, g.s), a.status);
+        c_win++;
+        c_smer++;
+        if (a.wend[pos]) {
+            c_sk++;
+            for (uint32_t u = 1; u <= ks; u++) {
+                insert_smer<BITS>(table32, g, base, canonical(codes64(a.codes, pos + u) & s_mask, g.s), a.status);
+                c_smer++;
+            }
+        }
+    }
+    warp_add_u64(&a.cnt[kCntWindows], c_win);
+    warp_add_u64(&a.cnt[kCntSmers], c_smer);
+    warp_add_u64(&a.cnt[kCntSuperKmers], c_sk);
+}
+
+template <int MODE, int BITS>
+__global__ void k_plain_query(TileArgs a) {
+    const DevGeom g = a.g;
+    unsigned long long c_valid = 0, c_pos = 0, c_sum = 0;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t n_iter = (a.n_bytes + stride - 1) / stride;
+    for (uint64_t it = 0; it < n_iter; it++) {
+        const uint64_t pos = it * stride + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+        if (pos >= a.n_bytes) continue;
+        const uint32_t blk = a.wblock[pos];
+        if (blk == 0xFFFFFFFFu) continue;
+        const uint32_t r = window_estimate<BITS>(a, g, a.codes, pos, block_base(g, blk));
+        if constexpr (MODE == kModeReport) {
+            c_valid++;
+            c_pos += r > 0;
+            c_sum += r;
+        } else {
+            const uint64_t j = seq_of(a.offsets, 0, a.n_seqs, pos);
+            const uint64_t o = a.woff[j] + (pos - __ldg(a.offsets + j));
+            a.out[o] = r;
+            a.out_valid[o] = 1;
+        }
+    }
+    warp_add_u64(&a.cnt[kCntValid], c_valid);
+    warp_add_u64(&a.cnt[kCntPositive], c_pos);
+    warp_add_u64(&a.cnt[kCntChecksum], c_sum);
+}
+
+static int plain_grid(uint64_t n) {
+    const uint64_t blocks = (n + 255) / 256;
+    return (int)(blocks < (1u << 20) ? (blocks ? blocks : 1) : (1u << 20));
+}
+
+void launch_plain_insert(const TileArgs& a, cudaStream_t st) {
+    const int grid = plain_grid(a.n_bytes);
+    switch (a.g.bits) {
+        case 8: k_plain_insert<8><<<grid, 256, 0, st>>>(a); break;
+        case 16: k_plain_insert<16><<<grid, 256, 0, st>>>(a); break;
+        default: k_plain_insert<32><<<grid, 256, 0, st>>>(a); break;
+    }
+    note_launch();
+}
+
+void launch_plain_query(int mode, const TileArgs& a, cudaStream_t st) {
+    const int grid = plain_grid(a.n_bytes);
+    if (mode == kModeReport) {
+        switch (a.g.bits) {
+            case 8: k_plain_query<kModeReport, 8><<<grid, 256, 0, st>>>(a); break;
+            case 16: k_plain_query<kModeReport, 16><<<grid, 256, 0, st>>>(a); break;
+            default: k_plain_query<kModeReport, 32><<<grid, 256, 0, st>>>(a); break;
+        }
+    } else {
+        switch (a.g.bits) {
+            case 8: k_plain_query<kModeAbund, 8><<<grid, 256, 0, st>>>(a); break;
+            case 16: k_plain_query<kModeAbund, 16><<<grid, 256, 0, st>>>(a); break;
+            default: k_plain_query<kModeAbund, 32><<<grid, 256, 0, st>>>(a); break;
+        }
+    }
+    note_launch();
+}
+
+// ---------------------------------------------------------------------------------------
+// Counter histogram (filter.rs:50-54, 267-275): value -> number of counters.
+// ---------------------------------------------------------------------------------------
+constexpr uint32_t kHistSmem = 8192;
+
+template <int BITS>
+__global__ void k_counter_hist(const void* __restrict__ table, uint64_t slots, unsigned long long* hist,
+                               uint32_t dense, unsigned long long* ovf, uint64_t ovf_cap,
+                               unsigned long long* ovf_count) {
+    __shared__ unsigned int sh[kHistSmem];
+    for (uint32_t i = threadIdx.x; i < kHistSmem; i += blockDim.x) sh[i] = 0;
+    __syncthreads();
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    const uint64_t wid = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    unsigned long long zeros = 0;
+    for (uint64_t base = wid * 32; base < slots; base += warps * 32) {
+        const uint64_t idx = base + lane;
+        const bool in = idx < slots;
+        const uint32_t v = in ? load_counter<BITS>(table, idx) : 0xFFFFFFFFu;
+        const bool is_zero = in && v == 0;
+        zeros += is_zero;
+        const bool other = in && v != 0;
+        const unsigned mask = __ballot_sync(0xFFFFFFFFu, other);
+        if (other) {
+            const unsigned peers = __match_any_sync(mask, v);
+            if (lane == (uint32_t)(__ffs(peers) - 1)) {
+                const unsigned c = __popc(peers);
+                if (v < kHistSmem) {
+                    atomicAdd(&sh[v], c);
+                } else if (v < dense) {
+                    atomicAdd(hist + v, (unsigned long long)c);
+                } else {
+                    const unsigned long long o = atomicAdd(ovf_count, (unsigned long long)c);
+                    for (unsigned q = 0; q < c; q++) {
+                        if (o + q < ovf_cap) ovf[o + q] = v;
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < kHistSmem; i += blockDim.x) {
+        if (sh[i]) atomicAdd(hist + i, (unsigned long long)sh[i]);
+    }
+    warp_add_u64(hist, zeros);
+}
+
+void launch_counter_hist(const void* table, uint64_t slots, int bits, unsigned long long* hist, uint32_t dense,
+                         unsigned long long* ovf, uint64_t ovf_cap, unsigned long long* ovf_count, cudaStream_t st) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const uint64_t want = (slots + 255) / 256;
+    const int grid = (int)(want < (uint64_t)sms * 4 ? (want ? want : 1) : (uint64_t)sms * 4);
+    switch (bits) {
+        case 8: k_counter_hist<8><<<grid, 256, 0, st>>>(table, slots, hist, dense, ovf, ovf_cap, ovf_count); break;
+        case 16: k_counter_hist<16><<<grid, 256, 0, st>>>(table, slots, hist, dense, ovf, ovf_cap, ovf_count); break;
+        default: k_counter_hist<32><<<grid, 256, 0, st>>>(table, slots, hist, dense, ovf, ovf_cap, ovf_count); break;
+    }
+    note_launch();
+}
+
+// ---------------------------------------------------------------------------------------
+// Small launches
+// ---------------------------------------------------------------------------------------
+__global__ void k_fill_u32(uint32_t* p, uint32_t v, uint64_t n) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) p[i] = v;
+}
+
+void launch_fill_u32(uint32_t* p, uint32_t v, uint64_t n, cudaStream_t st) {
+    if (n == 0) return;
+    const uint64_t blocks = (n + 255) / 256;
+    k_fill_u32<<<(unsigned)(blocks < 65536 ? blocks : 65536), 256, 0, st>>>(p, v, n);
+    note_launch();
+}
+
+void launch_pack(const uint8_t* ascii, uint64_t n_bytes, uint32_t* codes, uint32_t* valid, cudaStream_t st) {
+    const uint64_t n_groups = (n_bytes + 31) / 32;
+    if (n_groups == 0) return;
+    const int aligned = ((reinterpret_cast<uintptr_t>(ascii) & 15) == 0) ? 1 : 0;
+    const uint64_t blocks = (n_groups + 255) / 256;
+    k_pack<<<(unsigned)(blocks < (1u << 20) ? blocks : (1u << 20)), 256, 0, st>>>(ascii, n_bytes, codes, valid,
+                                                                                  n_groups, aligned);
+    note_launch();
+}
+
+void launch_seqstart(const uint64_t* offsets, uint64_t n_seqs, uint64_t n_bytes, uint32_t* seqstart,
+                     cudaStream_t st) {
+    if (n_seqs == 0) return;
+    const uint64_t blocks = (n_seqs + 255) / 256;
+    k_seqstart<<<(unsigned)(blocks < 65536 ? blocks : 65536), 256, 0, st>>>(offsets, n_seqs, n_bytes, seqstart);
+    note_launch();
+}
+
+void launch_seq_windows(const uint64_t* offsets, uint64_t n_seqs, uint32_t k, unsigned long long* cnt,
+                        uint64_t* woff, cudaStream_t st) {
+    if (n_seqs == 0) return;
+    const uint64_t blocks = (n_seqs + 255) / 256;
+    k_seq_windows<<<(unsigned)(blocks < 4096 ? blocks : 4096), 256, 0, st>>>(offsets, n_seqs, k, cnt, woff);
+    note_launch();
+}
+
+}  // namespace scb

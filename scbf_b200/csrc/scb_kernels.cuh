@@ -1,0 +1,95 @@
+// Kernel launch interface shared by the C ABI implementation (scb_api.cu) and the kernels
+// (scb_kernels.cu).  Host-only declarations; device code lives in scb_kernels.cu.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "scb_device.cuh"
+
+namespace scb {
+
+// Tile geometry of the fused kernels: windows per tile and threads per CTA.
+constexpr int kTileWindows = 1024;
+constexpr int kTileThreads = 256;
+
+enum TileMode : int {
+    kModeInsert = 0,       // (b)+(c)+(d): cut, hash, saturating insert
+    kModeReport = 1,       // (b)+(c)+(e): query, reduce to the QueryFastaReport fields
+    kModeAbund = 2,        // (b)+(c)+(e): query, per-window abundances
+    kModeDistinct = 3,     // (b)+(c)+(e)+(f): query, distinct-k-mer set and histogram
+    kModeStats = 4,        // super-k-mer / s-mer / sector counts
+    kModeDebugMin = 5,     // (b) only: chosen minimizer position per window
+    kModeMaterialize = 6,  // (b) for the plain pipeline: per-window block id + end flag in HBM
+    kModeInsertStaged = 7  // (b)+(c)+(d) with one warp per super-k-mer staging block deltas
+};
+
+// Slots of the per-launch 64-bit counter array.
+enum CounterSlot : int {
+    kCntWindows = 0,
+    kCntSmers = 1,
+    kCntValid = 2,
+    kCntPositive = 3,
+    kCntChecksum = 4,
+    kCntSuperKmers = 5,
+    kCntSectors = 6,
+    kCntDistinct = 7,
+    kCntOverflow = 8,
+    kCntRecords = 9,
+    kCntTotalWindows = 10,
+    kCntSlots = 16
+};
+
+struct TileArgs {
+    DevGeom g;
+    const uint32_t* codes;     // 2-bit codes (+ >= 4 zero words of padding)
+    const uint32_t* valid;     // valid bitmap (+ >= 4 zero words of padding)
+    const uint32_t* seqstart;  // sequence-start bitmap (+ padding)
+    uint64_t n_bytes;
+    uint64_t n_code_words;     // readable words (including padding)
+    uint64_t n_bit_words;
+    uint32_t n_tiles;
+    uint32_t pad_;
+    void* table;
+    uint32_t* status;
+    unsigned long long* cnt;   // kCntSlots counters
+    unsigned int* tile_counter;
+    // per-window abundances (kModeAbund)
+    const uint64_t* offsets;
+    uint64_t n_seqs;
+    const uint64_t* woff;      // first output window of each sequence
+    unsigned long long* out;
+    uint8_t* out_valid;
+    // distinct-k-mer spectrum (kModeDistinct)
+    unsigned long long* set_keys;
+    uint64_t set_mask;
+    unsigned long long* hist;  // dense bins [0, hist_dense)
+    uint32_t hist_dense;
+    uint32_t pad2_;
+    unsigned long long* ovf;   // values >= hist_dense of newly seen keys
+    uint64_t ovf_cap;
+    // plain pipeline (kModeMaterialize) and debug output
+    uint32_t* wblock;
+    uint8_t* wend;
+    uint32_t* dbg;
+};
+
+// Kernel launches; each counts itself in the library-wide launch counter.
+void launch_pack(const uint8_t* ascii, uint64_t n_bytes, uint32_t* codes, uint32_t* valid, cudaStream_t st);
+void launch_seqstart(const uint64_t* offsets, uint64_t n_seqs, uint64_t n_bytes, uint32_t* seqstart,
+                     cudaStream_t st);
+void launch_seq_windows(const uint64_t* offsets, uint64_t n_seqs, uint32_t k, unsigned long long* cnt,
+                        uint64_t* woff_or_null, cudaStream_t st);
+void launch_scan_inplace(uint64_t* data, uint64_t n, uint64_t* scratch, cudaStream_t st);
+void launch_tiles(int mode, const TileArgs& a, int grid, cudaStream_t st);
+int tile_grid(int mode, int bits, int sm_count, uint32_t n_tiles);
+void launch_plain_insert(const TileArgs& a, cudaStream_t st);
+void launch_plain_query(int mode, const TileArgs& a, cudaStream_t st);
+void launch_counter_hist(const void* table, uint64_t slots, int bits, unsigned long long* hist, uint32_t dense,
+                         unsigned long long* ovf, uint64_t ovf_cap, unsigned long long* ovf_count, cudaStream_t st);
+void launch_fill_u32(uint32_t* p, uint32_t v, uint64_t n, cudaStream_t st);
+
+uint64_t kernel_launch_count();
+void note_launch();
+
+}  // namespace scb
