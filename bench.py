@@ -53,6 +53,8 @@ def parse():
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--profile-case", choices=["plain", "fused", "grouped"], default=None,
+                   help="run one insert + query of a small case (for ncu) and exit")
     return p.parse_args()
 
 
@@ -214,6 +216,16 @@ def run_reference(args, dist: Dist):
 
 
 # ---------------------------------------------------------------------------------------
+STRATEGY_IDS = {"auto": 0, "plain": 1, "fused": 2, "grouped": 4}
+
+
+def occupied(n_items: float, n_bins: float) -> float:
+    """Expected number of distinct bins hit by n_items uniform draws over n_bins."""
+    if n_bins <= 0:
+        return 0.0
+    return n_bins * -np.expm1(-n_items / n_bins)
+
+
 def run_ours(args, dist: Dist):
     import torch
 
@@ -251,7 +263,9 @@ def run_ours(args, dist: Dist):
         check(L.scb_query_report_device(h, d_data.data_ptr(), d_off.data_ptr(), n_seqs, n_bytes, sp,
                                         C.byref(rep)))
 
-    def timed(steps: int) -> tuple[float, dict]:
+    def timed(strategy: str, steps: int) -> tuple[float, dict]:
+        sid = STRATEGY_IDS[strategy]
+        check(L.scb_set_strategy(h, sid, sid))
         for _ in range(args.warmup):
             step()
         torch.cuda.synchronize()
@@ -273,34 +287,36 @@ def run_ours(args, dist: Dist):
         t = _lib.ScbTimings()
         check(L.scb_get_timings(h, C.byref(t)))
         check(L.scb_set_timing(h, 0))
-        return dist.max(ms), {"clocks": clk, "launches": L.scb_kernel_launches() - launches0,
-                               "pack_ms": t.pack_ms / steps, "insert_ms": t.insert_ms / steps,
-                               "query_ms": t.query_ms / steps}
+        info = {"clocks": clk, "launches": L.scb_kernel_launches() - launches0}
+        for f in ("pack_ms", "insert_ms", "query_ms", "cut_ms", "bucket_ms", "apply_insert_ms", "apply_query_ms"):
+            info[f] = getattr(t, f) / steps
+        info["cut_ms"] /= 2  # one cut per insert and one per query
+        info["report"] = (rep.valid_kmers, rep.positive_estimates, rep.estimate_checksum)
+        return dist.max(ms), info
 
     # workload statistics for the algorithmic bytes (outside any timed region)
     st = _lib.ScbStats()
     check(L.scb_reset(h))
     check(L.scb_batch_stats(h, data.ctypes.data, offsets.ctypes.data, n_seqs, C.byref(st)))
 
-    check(L.scb_set_strategy(h, 2, 2))
-    ms, info = timed(args.steps)
+    ms, info = timed("auto", args.steps)
     kmers = km.value
     assert rep.valid_kmers == kmers, (rep.valid_kmers, kmers)
     all_kmers = dist.sum(float(kmers))
     value = all_kmers * args.steps / (ms / 1e3)
-    fused_report = (rep.valid_kmers, rep.positive_estimates, rep.estimate_checksum)
+    reference_report = info["report"]
 
+    strategies = {}
+    for name in ([] if args.no_plain else ["plain", "fused", "grouped"]):
+        s_steps = max(1, args.steps // 2)
+        sms, sinfo = timed(name, s_steps)
+        assert sinfo["report"] == reference_report, (name, sinfo["report"], reference_report)
+        strategies[name] = {"value": all_kmers * s_steps / (sms / 1e3), "ms_per_step": sms / s_steps,
+                            "insert_ms": sinfo["insert_ms"], "query_ms": sinfo["query_ms"]}
+    check(L.scb_set_strategy(h, 0, 0))
     plain = None
-    if not args.no_plain:
-        check(L.scb_set_strategy(h, 1, 1))
-        p_steps = max(1, args.steps // 2)
-        pms, pinfo = timed(p_steps)
-        assert (rep.valid_kmers, rep.positive_estimates, rep.estimate_checksum) == fused_report
-        pvalue = all_kmers * p_steps / (pms / 1e3)
-        plain = {"value": pvalue, "unit": "k-mers/s", "ms_per_step": pms / p_steps,
-                 "insert_ms": pinfo["insert_ms"], "query_ms": pinfo["query_ms"],
-                 "batched_over_plain": value / pvalue}
-        check(L.scb_set_strategy(h, 2, 2))
+    if "plain" in strategies:
+        plain = dict(strategies["plain"], unit="k-mers/s", batched_over_plain=value / strategies["plain"]["value"])
 
     e2e = None
     if not args.no_e2e:
@@ -317,25 +333,43 @@ def run_ours(args, dist: Dist):
             dt = time.perf_counter() - t0
             if i >= args.warmup:
                 times.append(dist.max(dt))
-        assert (rep.valid_kmers, rep.positive_estimates, rep.estimate_checksum) == fused_report
+        assert (rep.valid_kmers, rep.positive_estimates, rep.estimate_checksum) == reference_report
         e2e = {"value": all_kmers * len(times) / sum(times), "unit": "k-mers/s",
-               "h2d_bytes_per_step": n_bytes + (n_seqs + 1) * 8, "d2h_bytes_per_step": 2 * (16 * 8 + 4)}
+               "h2d_bytes_per_step": n_bytes + (n_seqs + 1) * 8, "d2h_bytes_per_step": 2 * (16 * 8 + 4) + 8}
 
-    # roofline of the dominant kernel (the insert tile kernel: one launch per step)
+    # roofline of the dominant kernel of the timed step
     peak, peak_kind = measured_peaks()
-    ins_bytes = 64 * st.sectors + n_bytes // 4
-    q_bytes = 32 * st.sectors + n_bytes // 4
-    dom = "insert" if info["insert_ms"] >= info["query_ms"] else "query"
-    dom_ms = info[f"{dom}_ms"]
-    alg = ins_bytes if dom == "insert" else q_bytes
-    achieved = alg / (dom_ms / 1e3) / 1e9
+    R = float(st.super_kmers)
+    bytes_per = GEOM["counter_bits"] // 8
+    block_bytes = (1 << GEOM["block_slots_exponent"]) * bytes_per
+    nb_blocks = 1 << (GEOM["counter_slots_exponent"] - GEOM["block_slots_exponent"])
+    touched = occupied(R, nb_blocks)
+    gather = (st.windows + R * (GEOM["k"] - 1)) / 4.0  # 2-bit bases of every record
+    kernels = {
+        # one read of the packed codes and bitmaps, 12-byte record and 8-byte bucket count per super-k-mer
+        "k_tiles<cut>": (info["cut_ms"], n_bytes / 2 + 20 * R),
+        # sorted records + gathered bases + each touched block read and written once
+        "k_apply<insert>": (info["apply_insert_ms"], 8 * R + gather + 2 * touched * block_bytes),
+        # sorted records + gathered bases + each touched block read once
+        "k_apply<query>": (info["apply_query_ms"], 8 * R + gather + touched * block_bytes),
+        # random-sector bound of the direct design: each distinct 32-byte sector read + written
+        "k_tiles<insert>": (info["insert_ms"] if info["cut_ms"] == 0 else 0.0, 64 * st.sectors + n_bytes / 4),
+    }
+    dom = max(kernels, key=lambda k_: kernels[k_][0])
+    dom_ms, alg = kernels[dom]
+    achieved = alg / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
     traffic = profile_traffic()
-    roofline = {"bound": "hbm", "kernel": f"k_tiles<{dom}>", "achieved": achieved, "peak": peak, "unit": "GB/s",
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_kind": peak_kind,
-                "traffic": (traffic["dram_bytes_per_kmer"] * kmers) if traffic else None,
+                "traffic": (traffic.get(dom, {}).get("dram_bytes_per_kmer", 0) * kmers) if traffic and dom in traffic
+                else None,
                 "algorithmic_bytes": alg, "kernel_ms": dom_ms,
+                "kernels_ms": {k_: v[0] for k_, v in kernels.items()},
+                "random_sector_bound_kmers_per_s": {
+                    "insert": kmers / ((64 * st.sectors + n_bytes / 4) / (peak * 1e9)),
+                    "query": kmers / ((32 * st.sectors + n_bytes / 4 + 8 * kmers) / (peak * 1e9))},
                 "sectors_per_superkmer": st.sectors / max(st.super_kmers, 1),
-                "super_kmers": st.super_kmers, "smers": st.smers}
+                "super_kmers": st.super_kmers, "smers": st.smers, "touched_blocks": touched}
 
     cpu = None
     if not args.no_cpu and dist.rank == 0 and dist.world == 1:
@@ -363,11 +397,12 @@ def run_ours(args, dist: Dist):
             "config": {"workload": WORKLOAD + (f" (genome scale {args.scale})" if args.scale != 1.0 else ""),
                        "reads": n_seqs, "bytes": n_bytes, "kmers_per_step": kmers,
                        "l2": "inputs larger than L2 (2 GB of reads, 2 GiB table)",
-                       "parallelism": f"replicas x{dist.world}", "strategy": "fused"},
+                       "parallelism": f"replicas x{dist.world}", "strategy": "auto"},
             "insert_kmers_per_s": kmers / (info["insert_ms"] / 1e3),
             "query_kmers_per_s": kmers / (info["query_ms"] / 1e3),
-            "stage_ms": {"pack": info["pack_ms"], "insert": info["insert_ms"], "query": info["query_ms"]},
-            "plain": plain, "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
+            "stage_ms": {k_: info[k_] for k_ in ("pack_ms", "insert_ms", "query_ms", "cut_ms", "bucket_ms",
+                                                 "apply_insert_ms", "apply_query_ms")},
+            "plain": plain, "strategies": strategies, "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
             "clocks": info["clocks"], "gpu_launches": info["launches"],
         }
         print(json.dumps(line), flush=True)
@@ -375,8 +410,43 @@ def run_ours(args, dist: Dist):
     ctx.close()
 
 
+def run_profile_case(args):
+    """One insert + one stream query of a small case (genome scale 0.1: 200 MB of reads, 2 GiB
+    table) with the chosen strategy: the command the ncu captures profile."""
+    import torch
+
+    from scbf_b200 import _lib, api
+
+    L = _lib.load()
+    data, offsets = workload(0, 0.1)
+    cfg = api.SuperCountingBloomConfig(k=GEOM["k"], m=GEOM["m"], s=GEOM["s"], n_hashes=GEOM["n_hashes"],
+                                       counter_bits=api.CounterBits(GEOM["counter_bits"]),
+                                       counter_slots_exponent=GEOM["counter_slots_exponent"],
+                                       block_slots_exponent=GEOM["block_slots_exponent"], threads=1, queue=4096)
+    ctx = api._create(cfg)
+    sid = STRATEGY_IDS[args.profile_case]
+    assert L.scb_set_strategy(ctx.h, sid, sid) == 0
+    d_data = torch.from_numpy(data).to("cuda")
+    d_off = torch.from_numpy(offsets.view(np.int64)).to("cuda")
+    km, sm = C.c_uint64(0), C.c_uint64(0)
+    rep = _lib.ScbReport()
+    n = len(offsets) - 1
+    assert L.scb_insert_batch_device(ctx.h, d_data.data_ptr(), d_off.data_ptr(), n, int(offsets[-1]), None,
+                                     C.byref(km), C.byref(sm)) == 0, _lib.last_error()
+    assert L.scb_freeze(ctx.h) == 0
+    assert L.scb_query_report_device(ctx.h, d_data.data_ptr(), d_off.data_ptr(), n, int(offsets[-1]), None,
+                                     C.byref(rep)) == 0, _lib.last_error()
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_case": args.profile_case, "kmers": km.value, "smers": sm.value,
+                      "checksum": rep.estimate_checksum}), flush=True)
+    ctx.close()
+
+
 def main():
     args = parse()
+    if args.profile_case:
+        run_profile_case(args)
+        return
     dist = Dist(args.gpus)
     try:
         if args.impl == "reference":

@@ -187,6 +187,11 @@ typedef struct scb_timings {
     double insert_ms;
     double query_ms;
     uint64_t batches;
+    /* grouped strategy breakdown (part of insert_ms / query_ms) */
+    double cut_ms;          /* kernel (b): records + bucket counts */
+    double bucket_ms;       /* bucket offsets, scatter, work items */
+    double apply_insert_ms; /* shared-memory insert apply kernel */
+    double apply_query_ms;  /* shared-memory query apply kernel */
 } scb_timings;
 scb_status scb_set_timing(scb_ctx* ctx, int enable); /* enabling also clears the totals */
 scb_status scb_get_timings(const scb_ctx* ctx, scb_timings* out);

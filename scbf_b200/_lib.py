@@ -41,7 +41,8 @@ class ScbStats(C.Structure):
 
 class ScbTimings(C.Structure):
     _fields_ = [("pack_ms", C.c_double), ("insert_ms", C.c_double), ("query_ms", C.c_double),
-                ("batches", C.c_uint64)]
+                ("batches", C.c_uint64), ("cut_ms", C.c_double), ("bucket_ms", C.c_double),
+                ("apply_insert_ms", C.c_double), ("apply_query_ms", C.c_double)]
 
 
 _lib = None

@@ -92,11 +92,15 @@ constexpr uint64_t kPadWords = 16;
 // Derived per-batch arrays (codes, bitmaps, window offsets, plain-pipeline arrays, counters).
 struct Lane {
     DevBuf ascii, offsets, codes, valid, seqstart, woff, scan, wblock, wend, cnt, tiles;
+    // grouped pipeline: records, bucket offsets / cursors, work items
+    DevBuf rec_key, rec_val, rec_sorted, bhist, bcursor, icount, items, gscan, rec_count;
     cudaStream_t stream = nullptr;
-    // stage timing: [0,1] pack, [2,3] main stage; main_kind 1 = insert, 2 = query
-    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    // stage timing: [0,1] pack, [2,3] main stage (main_kind 1 = insert, 2 = query),
+    // [4,5,6,7] grouped cut start / cut end / apply start / apply end (grouped_kind as main_kind)
+    cudaEvent_t ev[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     bool pack_timed = false;
     int main_kind = 0;
+    int grouped_kind = 0;
     ~Lane() {
         for (auto& e : ev) {
             if (e) cudaEventDestroy(e);
@@ -292,9 +296,30 @@ scb_status prepare_batch(scb_ctx* ctx, Lane& L, const uint8_t* d_ascii, const ui
     return SCB_OK;
 }
 
-scb_strategy resolve(scb_strategy s) {
-    if (s == SCB_STRATEGY_PLAIN) return SCB_STRATEGY_PLAIN;
+bool grouped_supported(const scb_ctx* ctx) { return ctx->block_slots <= kMaxBucketSlots; }
+
+// Expected super-k-mer records of a batch: about 2/(w+1) per window (random minimizers).
+uint64_t records_estimate(const scb_ctx* ctx, uint64_t n_bytes) { return n_bytes * 2 / (ctx->g.w + 1) + 1; }
+
+scb_strategy resolve(const scb_ctx* ctx, scb_strategy s, uint64_t n_bytes) {
+    if (s == SCB_STRATEGY_PLAIN || s == SCB_STRATEGY_FUSED) return s;
+    if (s == SCB_STRATEGY_GROUPED) return grouped_supported(ctx) ? s : SCB_STRATEGY_FUSED;
+    // auto: grouping pays once a batch brings several super-k-mers per touched block
+    if (grouped_supported(ctx) && records_estimate(ctx, n_bytes) >= ctx->nb_blocks / 2) return SCB_STRATEGY_GROUPED;
     return SCB_STRATEGY_FUSED;
+}
+
+scb_strategy resolve(scb_strategy s) { return s == SCB_STRATEGY_AUTO ? SCB_STRATEGY_FUSED : s; }
+
+// Buckets of 2^shift consecutive blocks: about 512 records per bucket, at most 4096 counters
+// (or one block when blocks are larger) staged in shared memory.
+uint32_t bucket_shift_for(const scb_ctx* ctx, uint64_t records) {
+    uint32_t shift = 0;
+    while ((ctx->block_slots << (shift + 1)) <= 4096 && (1ull << (shift + 1)) <= ctx->nb_blocks &&
+           records * (1ull << shift) / ctx->nb_blocks < 512) {
+        shift++;
+    }
+    return shift;
 }
 
 scb_status run_tiles(scb_ctx* ctx, Lane& L, int mode, TileArgs& a, cudaStream_t st) {
@@ -315,8 +340,83 @@ scb_status run_materialize(scb_ctx* ctx, Lane& L, TileArgs& a, cudaStream_t st) 
     return run_tiles(ctx, L, kModeMaterialize, a, st);
 }
 
+// Grouped pipeline for one batch: cut into records, bucket them by block, build work items and
+// run the shared-memory apply kernel (insert or report query).
+scb_status run_grouped(scb_ctx* ctx, Lane& L, int mode, TileArgs& a, cudaStream_t st) {
+    if (a.n_tiles == 0) return SCB_OK;
+    uint64_t cap = records_estimate(ctx, a.n_bytes) * 5 / 4 + 65536;
+    const uint32_t shift = bucket_shift_for(ctx, records_estimate(ctx, a.n_bytes));
+    const uint64_t n_buckets = ctx->nb_blocks >> shift;
+    SCB_TRY(L.bhist.ensure((n_buckets + 1) * 8));
+    SCB_TRY(L.bcursor.ensure((n_buckets + 1) * 8));
+    SCB_TRY(L.icount.ensure((n_buckets + 1) * 8));
+    SCB_TRY(L.gscan.ensure(((n_buckets + 1) / 1024 + 64) * 8 * 2));
+    SCB_TRY(L.rec_count.ensure(64));
+    unsigned long long produced = 0;
+    if (ctx->timing) SCB_CUDA(cudaEventRecord(L.ev[4], st));
+    for (int attempt = 0; attempt < 2; attempt++) {
+        SCB_TRY(L.rec_key.ensure(cap * 4));
+        SCB_TRY(L.rec_val.ensure(cap * 8));
+        SCB_CUDA(cudaMemsetAsync(L.bhist.p, 0, (n_buckets + 1) * 8, st));
+        SCB_CUDA(cudaMemsetAsync(L.rec_count.p, 0, 8, st));
+        a.rec_key = L.rec_key.as<uint32_t>();
+        a.rec_val = L.rec_val.as<unsigned long long>();
+        a.rec_count = L.rec_count.as<unsigned long long>();
+        a.rec_cap = cap;
+        a.bucket_hist = L.bhist.as<unsigned long long>();
+        a.bucket_shift = shift;
+        if (attempt == 1) {  // the cut's own counters only (windows, s-mers, super-k-mers)
+            SCB_CUDA(cudaMemsetAsync(a.cnt + kCntWindows, 0, 8, st));
+            SCB_CUDA(cudaMemsetAsync(a.cnt + kCntSmers, 0, 8, st));
+            SCB_CUDA(cudaMemsetAsync(a.cnt + kCntSuperKmers, 0, 8, st));
+        }
+        SCB_TRY(run_tiles(ctx, L, kModeCut, a, st));
+        if (ctx->timing) SCB_CUDA(cudaEventRecord(L.ev[5], st));
+        SCB_CUDA(cudaMemcpyAsync(&produced, L.rec_count.p, 8, cudaMemcpyDeviceToHost, st));
+        SCB_CUDA(cudaStreamSynchronize(st));
+        if (produced <= cap) break;
+        cap = produced + 1024;  // more super-k-mers than estimated: size exactly and cut again
+    }
+    if (produced > cap) return fail_kind(SCB_ERR_INTERNAL_STATE, "super-k-mer record overflow");
+    if (produced == 0) return SCB_OK;
+    SCB_TRY(L.rec_sorted.ensure(produced * 8));
+    launch_scan_inplace(reinterpret_cast<uint64_t*>(L.bhist.p), n_buckets + 1, L.gscan.as<uint64_t>(), st);
+    SCB_CUDA(cudaMemcpyAsync(L.bcursor.p, L.bhist.p, (n_buckets + 1) * 8, cudaMemcpyDeviceToDevice, st));
+    launch_scatter(a.rec_key, a.rec_val, a.rec_count, cap, shift, L.bcursor.as<unsigned long long>(),
+                   L.rec_sorted.as<unsigned long long>(), st);
+    launch_item_counts(L.bhist.as<unsigned long long>(), n_buckets, L.icount.as<uint64_t>(), st);
+    launch_scan_inplace(L.icount.as<uint64_t>(), n_buckets + 1, L.gscan.as<uint64_t>(), st);
+    const uint64_t max_items = std::min<uint64_t>(n_buckets, produced) + produced / kItemRecords + 1;
+    SCB_TRY(L.items.ensure(max_items * 16));
+    launch_item_write(L.bhist.as<unsigned long long>(), L.icount.as<uint64_t>(), n_buckets, L.items.as<uint4>(), st);
+    GroupArgs ga;
+    std::memset(&ga, 0, sizeof(ga));
+    ga.g = ctx->g;
+    ga.codes = a.codes;
+    ga.n_code_words = a.n_code_words;
+    ga.table = ctx->table;
+    ga.status = ctx->status;
+    ga.cnt = a.cnt;
+    ga.recs = L.rec_sorted.as<unsigned long long>();
+    ga.items = L.items.as<uint4>();
+    ga.n_items = reinterpret_cast<const unsigned long long*>(L.icount.as<uint64_t>() + n_buckets);
+    ga.work_counter = L.tiles.as<unsigned int>() + 1;
+    ga.bucket_shift = shift;
+    SCB_CUDA(cudaMemsetAsync(ga.work_counter, 0, 4, st));
+    if (ctx->timing) SCB_CUDA(cudaEventRecord(L.ev[6], st));
+    launch_apply(mode, ga, (int)ctx->cfg.block_slots_exponent, 1u << shift, ctx->sm_count, max_items, st);
+    SCB_CUDA(cudaGetLastError());
+    if (ctx->timing) {
+        SCB_CUDA(cudaEventRecord(L.ev[7], st));
+        L.grouped_kind = mode == kModeInsert ? 1 : 2;
+    }
+    return SCB_OK;
+}
+
 scb_status insert_stage(scb_ctx* ctx, Lane& L, TileArgs& a, cudaStream_t st) {
-    if (resolve(ctx->insert_strategy) == SCB_STRATEGY_PLAIN) {
+    const scb_strategy s = resolve(ctx, ctx->insert_strategy, a.n_bytes);
+    if (s == SCB_STRATEGY_GROUPED) return run_grouped(ctx, L, kModeInsert, a, st);
+    if (s == SCB_STRATEGY_PLAIN) {
         SCB_TRY(run_materialize(ctx, L, a, st));
         launch_plain_insert(a, st);
         SCB_CUDA(cudaGetLastError());
@@ -326,7 +426,9 @@ scb_status insert_stage(scb_ctx* ctx, Lane& L, TileArgs& a, cudaStream_t st) {
 }
 
 scb_status query_stage(scb_ctx* ctx, Lane& L, int mode, TileArgs& a, cudaStream_t st) {
-    if (resolve(ctx->query_strategy) == SCB_STRATEGY_PLAIN && (mode == kModeReport || mode == kModeAbund)) {
+    const scb_strategy s = resolve(ctx, ctx->query_strategy, a.n_bytes);
+    if (s == SCB_STRATEGY_GROUPED && mode == kModeReport) return run_grouped(ctx, L, kModeReport, a, st);
+    if (s == SCB_STRATEGY_PLAIN && (mode == kModeReport || mode == kModeAbund)) {
         SCB_TRY(run_materialize(ctx, L, a, st));
         launch_plain_query(mode, a, st);
         SCB_CUDA(cudaGetLastError());
@@ -367,9 +469,17 @@ scb_status read_counters(scb_ctx* ctx, Lane& L, cudaStream_t st, unsigned long l
         if (L.main_kind && cudaEventElapsedTime(&ms, L.ev[2], L.ev[3]) == cudaSuccess) {
             (L.main_kind == 1 ? ctx->times.insert_ms : ctx->times.query_ms) += ms;
         }
+        if (L.grouped_kind) {
+            if (cudaEventElapsedTime(&ms, L.ev[4], L.ev[5]) == cudaSuccess) ctx->times.cut_ms += ms;
+            if (cudaEventElapsedTime(&ms, L.ev[5], L.ev[6]) == cudaSuccess) ctx->times.bucket_ms += ms;
+            if (cudaEventElapsedTime(&ms, L.ev[6], L.ev[7]) == cudaSuccess) {
+                (L.grouped_kind == 1 ? ctx->times.apply_insert_ms : ctx->times.apply_query_ms) += ms;
+            }
+        }
         if (L.pack_timed || L.main_kind) ctx->times.batches++;
         L.pack_timed = false;
         L.main_kind = 0;
+        L.grouped_kind = 0;
     }
     if (status) {
         return fail_kind(SCB_ERR_INTERNAL_STATE, "device status word 0x" + std::to_string(status) +

@@ -247,7 +247,9 @@ __global__ void __launch_bounds__(kTileThreads) k_tiles(TileArgs a) {
         const uint32_t tile = sm.tile;
         if (tile >= a.n_tiles) break;
         const uint64_t t0 = (uint64_t)tile * kTileWindows;
-        const uint32_t back = (MODE == kModeStats) ? (uint32_t)(t0 < (uint64_t)kBack ? t0 : (uint64_t)kBack) : 0u;
+        const uint32_t back = (MODE == kModeStats || MODE == kModeCut)
+                                  ? (uint32_t)(t0 < (uint64_t)kBack ? t0 : (uint64_t)kBack)
+                                  : 0u;
         const uint64_t e0 = t0 - back;
         const uint32_t n_eval = back + kTileWindows + kFwd;
         const uint32_t n_keys = n_eval + g.w - 1;
@@ -408,6 +410,41 @@ __global__ void __launch_bounds__(kTileThreads) k_tiles(TileArgs a) {
                     c_sec += (unsigned long long)n_sm * g.h;
                 }
             }
+        } else if constexpr (MODE == kModeCut) {
+            // one record per super-k-mer, emitted at its last window: (block, first window, windows)
+            const uint32_t lane = tid & 31;
+            for (uint32_t r = 0; r < kTileWindows / kTileThreads; r++) {
+                const uint32_t i = back + r * kTileThreads + tid;
+                const uint16_t po = sm.poff[i];
+                const bool valid = po != kNoWindow;
+                const bool end = valid && sm.poff[i + 1] != po;
+                uint32_t st = i;
+                if (end) {
+                    while (st > 0 && sm.poff[st - 1] == po) st--;
+                }
+                const uint32_t nwin = i - st + 1;
+                c_win += valid;
+                if (end) {
+                    c_sk++;
+                    c_smer += nwin + ks;
+                }
+                const unsigned mask = __ballot_sync(0xFFFFFFFFu, end);
+                unsigned long long base = 0;
+                if (mask) {
+                    const int leader = __ffs(mask) - 1;
+                    if ((int)lane == leader) base = atomicAdd(a.rec_count, (unsigned long long)__popc(mask));
+                    base = __shfl_sync(0xFFFFFFFFu, base, leader);
+                }
+                if (end) {
+                    const unsigned long long slot = base + __popc(mask & ((1u << lane) - 1u));
+                    const uint32_t block = sm.block[i];
+                    if (slot < a.rec_cap) {
+                        a.rec_key[slot] = block;
+                        a.rec_val[slot] = (unsigned long long)(e0 + st) | ((unsigned long long)nwin << kRecWindowsShift);
+                    }
+                    atomicAdd(a.bucket_hist + (block >> a.bucket_shift), 1ull);
+                }
+            }
         } else if constexpr (MODE == kModeDebugMin) {
             for (uint32_t i = tid; i < kTileWindows; i += blockDim.x) {
                 const uint64_t pos = t0 + i;
@@ -454,6 +491,7 @@ void launch_tiles(int mode, const TileArgs& a, int grid, cudaStream_t st) {
         case kModeStats: launch_tiles_bits<kModeStats>(a, grid, st); break;
         case kModeDebugMin: launch_tiles_bits<kModeDebugMin>(a, grid, st); break;
         case kModeMaterialize: launch_tiles_bits<kModeMaterialize>(a, grid, st); break;
+        case kModeCut: launch_tiles_bits<kModeCut>(a, grid, st); break;
         default: break;
     }
 }
@@ -471,6 +509,7 @@ int tile_grid(int mode, int bits, int sm_count, uint32_t n_tiles) {
         case kModeDistinct: SCB_PICK(kModeDistinct); break;
         case kModeStats: SCB_PICK(kModeStats); break;
         case kModeDebugMin: SCB_PICK(kModeDebugMin); break;
+        case kModeCut: SCB_PICK(kModeCut); break;
         default: SCB_PICK(kModeMaterialize); break;
     }
 #undef SCB_PICK
@@ -636,6 +675,311 @@ void launch_counter_hist(const void* table, uint64_t slots, int bits, unsigned l
         case 16: k_counter_hist<16><<<grid, 256, 0, st>>>(table, slots, hist, dense, ovf, ovf_cap, ovf_count); break;
         default: k_counter_hist<32><<<grid, 256, 0, st>>>(table, slots, hist, dense, ovf, ovf_cap, ovf_count); break;
     }
+    note_launch();
+}
+
+// ---------------------------------------------------------------------------------------
+// Grouped pipeline: records bucketed by block; each work item's blocks live in shared memory.
+// ---------------------------------------------------------------------------------------
+__global__ void k_scatter(const uint32_t* __restrict__ key, const unsigned long long* __restrict__ val,
+                          const unsigned long long* __restrict__ count, uint64_t cap, uint32_t shift,
+                          unsigned long long* __restrict__ cursor, unsigned long long* __restrict__ sorted) {
+    const uint64_t n = min((uint64_t)*count, cap);
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const uint32_t local_mask = (1u << shift) - 1u;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const uint32_t block = key[i];
+        const unsigned long long pos = atomicAdd(cursor + (block >> shift), 1ull);
+        sorted[pos] = val[i] | ((unsigned long long)(block & local_mask) << kRecLocalShift);
+    }
+}
+
+__global__ void k_item_counts(const unsigned long long* __restrict__ off, uint64_t n_buckets,
+                              uint64_t* __restrict__ item_count) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; b <= n_buckets; b += stride) {
+        if (b == n_buckets) {
+            item_count[b] = 0;
+        } else {
+            const uint64_t c = off[b + 1] - off[b];
+            item_count[b] = (c + kItemRecords - 1) / kItemRecords;
+        }
+    }
+}
+
+__global__ void k_item_write(const unsigned long long* __restrict__ off, const uint64_t* __restrict__ item_off,
+                             uint64_t n_buckets, uint4* __restrict__ items) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; b < n_buckets; b += stride) {
+        const uint64_t c = off[b + 1] - off[b];
+        const uint64_t ni = item_off[b + 1] - item_off[b];
+        for (uint64_t t = 0; t < ni; t++) {
+            const uint64_t first = off[b] + t * kItemRecords;
+            const uint64_t cnt = min((uint64_t)kItemRecords, c - t * kItemRecords);
+            items[item_off[b] + t] = make_uint4((uint32_t)b, (uint32_t)first, (uint32_t)cnt, ni == 1 ? 1u : 0u);
+        }
+    }
+}
+
+// Largest r in [0, n) with pre[r] <= v (pre[0] = 0, pre non-decreasing).
+__device__ __forceinline__ uint32_t find_rec(const uint32_t* pre, uint32_t n, uint32_t v) {
+    uint32_t lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (pre[mid] <= v) {
+            lo = mid;
+        } else {
+            hi = mid - 1;
+        }
+    }
+    return lo;
+}
+
+__device__ __forceinline__ uint64_t codes64_ldg(const uint32_t* words, uint64_t b) {
+    const uint64_t w = b >> 4;
+    const uint32_t sh = (uint32_t)(b & 15) * 2u;
+    const uint32_t w0 = __ldg(words + w), w1 = __ldg(words + w + 1), w2 = __ldg(words + w + 2);
+    return ((uint64_t)__funnelshift_r(w1, w2, sh) << 32) | __funnelshift_r(w0, w1, sh);
+}
+
+// Block-wide exclusive prefix of (n_r + ks) and n_r over the chunk's records into spre / wpre.
+__device__ __forceinline__ void chunk_prefix(const unsigned long long* rv, uint32_t nrec, uint32_t ks, uint32_t* spre,
+                                             uint32_t* wpre, uint32_t* warp_tot) {
+    const uint32_t tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    uint32_t w = 0;
+    if (tid < nrec) w = (uint32_t)((rv[tid] >> kRecWindowsShift) & 63u);
+    const uint32_t s = tid < nrec ? w + ks : 0u;
+    uint32_t pack_s = s, pack_w = w;
+    for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t ys = __shfl_up_sync(0xFFFFFFFFu, pack_s, off);
+        const uint32_t yw = __shfl_up_sync(0xFFFFFFFFu, pack_w, off);
+        if ((int)lane >= off) {
+            pack_s += ys;
+            pack_w += yw;
+        }
+    }
+    if (lane == 31) {
+        warp_tot[2 * wid] = pack_s;
+        warp_tot[2 * wid + 1] = pack_w;
+    }
+    __syncthreads();
+    uint32_t add_s = 0, add_w = 0;
+    for (uint32_t x = 0; x < wid; x++) {
+        add_s += warp_tot[2 * x];
+        add_w += warp_tot[2 * x + 1];
+    }
+    if (tid < nrec) {
+        spre[tid + 1] = pack_s + add_s;
+        wpre[tid + 1] = pack_w + add_w;
+    }
+    if (tid == 0) {
+        spre[0] = 0;
+        wpre[0] = 0;
+    }
+    __syncthreads();
+}
+
+template <int MODE, int BITS>
+__global__ void __launch_bounds__(kTileThreads) k_apply(GroupArgs a, uint32_t bs_log2, uint32_t bucket_blocks) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    using T = CounterTraits<BITS>;
+    const DevGeom g = a.g;
+    const uint32_t bs = 1u << bs_log2;
+    const uint32_t bucket_slots = bs * bucket_blocks;
+    uint32_t* cells = reinterpret_cast<uint32_t*>(smem_raw);
+    unsigned long long* rv = reinterpret_cast<unsigned long long*>(cells + ((bucket_slots + 3u) & ~3u));
+    uint32_t* spre = reinterpret_cast<uint32_t*>(rv + kApplyChunk);
+    uint32_t* wpre = spre + kApplyChunk + 4;
+    uint8_t* touched = reinterpret_cast<uint8_t*>(wpre + kApplyChunk + 4);
+    uint32_t* est = reinterpret_cast<uint32_t*>(touched + ((bucket_blocks + 15u) & ~15u));
+    __shared__ uint4 item;
+    __shared__ uint32_t warp_tot[2 * (kTileThreads / 32)];
+
+    const uint32_t tid = threadIdx.x;
+    const uint32_t ks = g.k - g.s;
+    const uint64_t s_mask = len_mask(g.s);
+    uint32_t* table32 = reinterpret_cast<uint32_t*>(a.table);
+    const uint64_t n_items = *a.n_items;
+    unsigned long long c_valid = 0, c_pos = 0, c_sum = 0;
+
+    while (true) {
+        if (tid == 0) {
+            const unsigned idx = atomicAdd(a.work_counter, 1u);
+            item = idx < n_items ? a.items[idx] : make_uint4(0xFFFFFFFFu, 0, 0, 0);
+        }
+        __syncthreads();
+        const uint4 it = item;
+        if (it.x == 0xFFFFFFFFu) break;
+        const uint64_t bucket = it.x;
+        const uint64_t first = it.y;
+        const uint32_t count = it.z;
+        const bool exclusive = it.w != 0;
+
+        for (uint32_t x = tid; x < bucket_blocks; x += blockDim.x) touched[x] = 0;
+        if constexpr (MODE == kModeInsert) {
+            for (uint32_t x = tid; x < bucket_slots; x += blockDim.x) cells[x] = 0;
+        }
+        __syncthreads();
+        if constexpr (MODE == kModeReport) {
+            // stage the counters of the blocks this item reads
+            for (uint32_t r = tid; r < count; r += blockDim.x) touched[a.recs[first + r] >> kRecLocalShift] = 1;
+            __syncthreads();
+            for (uint32_t x = tid; x < bucket_slots; x += blockDim.x) {
+                const uint32_t lb = x >> bs_log2;
+                if (!touched[lb]) continue;
+                const uint64_t base = block_base(g, (bucket << a.bucket_shift) | lb);
+                cells[x] = load_counter<BITS>(a.table, base + (x & (bs - 1)));
+            }
+            __syncthreads();
+        }
+
+        for (uint32_t c0 = 0; c0 < count; c0 += kApplyChunk) {
+            const uint32_t nrec = min(kApplyChunk, count - c0);
+            if (tid < nrec) rv[tid] = a.recs[first + c0 + tid];
+            __syncthreads();
+            chunk_prefix(rv, nrec, ks, spre, wpre, warp_tot);
+            const uint32_t S = spre[nrec];
+            for (uint32_t f = tid; f < S; f += blockDim.x) {
+                const uint32_t r = find_rec(spre, nrec, f);
+                const unsigned long long v = rv[r];
+                const uint64_t pos = (uint32_t)v + (f - spre[r]);
+                const uint32_t lb = (uint32_t)(v >> kRecLocalShift);
+                const uint64_t smer = canonical(codes64_ldg(a.codes, pos) & s_mask, g.s);
+                uint64_t hash = xorshift64(smer);
+                uint32_t* blk = cells + (lb << bs_log2);
+                if constexpr (MODE == kModeInsert) {
+                    for (uint32_t h = 0; h < g.h; h++) {
+                        atomicAdd(blk + (hash & g.bs_mask), 1u);
+                        hash = xorshift64(hash);
+                    }
+                    touched[lb] = 1;
+                } else {
+                    uint32_t e = T::kMax;
+                    for (uint32_t h = 0; h < g.h; h++) {
+                        const uint32_t c = blk[hash & g.bs_mask];
+                        e = c < e ? c : e;
+                        hash = xorshift64(hash);
+                    }
+                    est[f] = e;
+                }
+            }
+            __syncthreads();
+            if constexpr (MODE == kModeReport) {
+                const uint32_t W = wpre[nrec];
+                for (uint32_t v = tid; v < W; v += blockDim.x) {
+                    const uint32_t r = find_rec(wpre, nrec, v);
+                    const uint32_t j = v - wpre[r];
+                    const uint32_t* e = est + spre[r] + j;
+                    uint32_t m = e[0];
+                    for (uint32_t t = 1; t <= ks; t++) m = e[t] < m ? e[t] : m;
+                    c_valid++;
+                    c_pos += m > 0;
+                    c_sum += m;
+                }
+                __syncthreads();
+            }
+        }
+
+        if constexpr (MODE == kModeInsert) {
+            // commit the deltas: min(old + delta, MAX) per counter (counter.rs saturation)
+            constexpr uint32_t lanes = T::kLanes;
+            const bool word_ok = exclusive && (bs % lanes) == 0;
+            if (word_ok) {
+                const uint32_t block_words = bs / lanes;
+                for (uint32_t x = tid; x < bucket_blocks * block_words; x += blockDim.x) {
+                    const uint32_t lb = x / block_words, wi = x % block_words;
+                    if (!touched[lb]) continue;
+                    const uint64_t base = block_base(g, (bucket << a.bucket_shift) | lb);
+                    uint32_t* wp = table32 + base / lanes + wi;
+                    const uint32_t old = __ldcg(wp);
+                    uint32_t nw = 0;
+#pragma unroll
+                    for (uint32_t l = 0; l < lanes; l++) {
+                        const uint64_t cur = (old >> (l * BITS)) & T::kMax;
+                        const uint64_t sum = cur + cells[(lb << bs_log2) + wi * lanes + l];
+                        nw |= (uint32_t)(sum < T::kMax ? sum : T::kMax) << (l * BITS);
+                    }
+                    __stcg(wp, nw);
+                }
+            } else {
+                for (uint32_t x = tid; x < bucket_slots; x += blockDim.x) {
+                    const uint32_t lb = x >> bs_log2;
+                    const uint32_t d = cells[x];
+                    if (!touched[lb] || d == 0) continue;
+                    const uint64_t base = block_base(g, (bucket << a.bucket_shift) | lb);
+                    sat_add<BITS>(table32, base + (x & (bs - 1)), d, a.status);
+                }
+            }
+        }
+        __syncthreads();
+    }
+    warp_add_u64(&a.cnt[kCntValid], c_valid);
+    warp_add_u64(&a.cnt[kCntPositive], c_pos);
+    warp_add_u64(&a.cnt[kCntChecksum], c_sum);
+}
+
+static size_t apply_smem(int mode, uint32_t bucket_slots, uint32_t bucket_blocks) {
+    size_t b = ((bucket_slots + 3u) & ~3u) * 4u + kApplyChunk * 8u + 2u * (kApplyChunk + 4u) * 4u +
+               ((bucket_blocks + 15u) & ~15u);
+    if (mode == kModeReport) b += (size_t)kApplyChunk * 64u * 4u;
+    return b;
+}
+
+template <int MODE, int BITS>
+static void launch_apply_t(const GroupArgs& a, int bs_log2, uint32_t bucket_blocks, int sm_count, uint64_t max_items,
+                           cudaStream_t st) {
+    const size_t smem = apply_smem(MODE, (1u << bs_log2) * bucket_blocks, bucket_blocks);
+    auto fn = k_apply<MODE, BITS>;
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int per_sm = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kTileThreads, smem) != cudaSuccess || per_sm < 1) {
+        per_sm = 1;
+    }
+    uint64_t grid = (uint64_t)per_sm * sm_count;
+    if (grid > max_items) grid = max_items;
+    if (grid == 0) grid = 1;
+    fn<<<(unsigned)grid, kTileThreads, smem, st>>>(a, (uint32_t)bs_log2, bucket_blocks);
+    note_launch();
+}
+
+void launch_apply(int mode, const GroupArgs& a, int bs_log2, uint32_t bucket_blocks, int sm_count, uint64_t max_items,
+                  cudaStream_t st) {
+    if (mode == kModeInsert) {
+        switch (a.g.bits) {
+            case 8: launch_apply_t<kModeInsert, 8>(a, bs_log2, bucket_blocks, sm_count, max_items, st); break;
+            case 16: launch_apply_t<kModeInsert, 16>(a, bs_log2, bucket_blocks, sm_count, max_items, st); break;
+            default: launch_apply_t<kModeInsert, 32>(a, bs_log2, bucket_blocks, sm_count, max_items, st); break;
+        }
+    } else {
+        switch (a.g.bits) {
+            case 8: launch_apply_t<kModeReport, 8>(a, bs_log2, bucket_blocks, sm_count, max_items, st); break;
+            case 16: launch_apply_t<kModeReport, 16>(a, bs_log2, bucket_blocks, sm_count, max_items, st); break;
+            default: launch_apply_t<kModeReport, 32>(a, bs_log2, bucket_blocks, sm_count, max_items, st); break;
+        }
+    }
+}
+
+void launch_scatter(const uint32_t* rec_key, const unsigned long long* rec_val, const unsigned long long* rec_count,
+                    uint64_t rec_cap, uint32_t bucket_shift, unsigned long long* cursor, unsigned long long* sorted,
+                    cudaStream_t st) {
+    const uint64_t blocks = (rec_cap + 255) / 256;
+    k_scatter<<<(unsigned)(blocks < 16384 ? (blocks ? blocks : 1) : 16384), 256, 0, st>>>(
+        rec_key, rec_val, rec_count, rec_cap, bucket_shift, cursor, sorted);
+    note_launch();
+}
+
+void launch_item_counts(const unsigned long long* bucket_off, uint64_t n_buckets, uint64_t* item_count,
+                        cudaStream_t st) {
+    const uint64_t blocks = (n_buckets + 1 + 255) / 256;
+    k_item_counts<<<(unsigned)(blocks < 16384 ? blocks : 16384), 256, 0, st>>>(bucket_off, n_buckets, item_count);
+    note_launch();
+}
+
+void launch_item_write(const unsigned long long* bucket_off, const uint64_t* item_off, uint64_t n_buckets,
+                       uint4* items, cudaStream_t st) {
+    const uint64_t blocks = (n_buckets + 255) / 256;
+    k_item_write<<<(unsigned)(blocks < 16384 ? (blocks ? blocks : 1) : 16384), 256, 0, st>>>(bucket_off, item_off,
+                                                                                           n_buckets, items);
     note_launch();
 }
 

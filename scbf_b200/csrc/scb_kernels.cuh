@@ -21,7 +21,32 @@ enum TileMode : int {
     kModeStats = 4,        // super-k-mer / s-mer / sector counts
     kModeDebugMin = 5,     // (b) only: chosen minimizer position per window
     kModeMaterialize = 6,  // (b) for the plain pipeline: per-window block id + end flag in HBM
-    kModeInsertStaged = 7  // (b)+(c)+(d) with one warp per super-k-mer staging block deltas
+    kModeInsertStaged = 7, // (b)+(c)+(d) with one warp per super-k-mer staging block deltas
+    kModeCut = 8           // (b) for the grouped pipeline: one record per super-k-mer + bucket counts
+};
+
+// Grouped pipeline: super-k-mer records bucketed by counter block.
+// Unsorted record: key = block id, val = first window position | windows << 32.
+// Sorted record:   val = first window position | windows << 32 | block-in-bucket << 38.
+constexpr uint32_t kRecWindowsShift = 32;
+constexpr uint32_t kRecLocalShift = 38;
+constexpr uint32_t kItemRecords = 4096;    // records per work item (heavier buckets are split)
+constexpr uint32_t kApplyChunk = 128;      // records staged in shared memory at a time
+constexpr uint32_t kMaxBucketSlots = 16384;  // counters of one bucket held in shared memory
+
+struct GroupArgs {
+    DevGeom g;
+    const uint32_t* codes;
+    uint64_t n_code_words;
+    void* table;
+    uint32_t* status;
+    unsigned long long* cnt;
+    const unsigned long long* recs;  // sorted records
+    const uint4* items;              // {bucket, first record, records, exclusive}
+    const unsigned long long* n_items;
+    unsigned int* work_counter;
+    uint32_t bucket_shift;
+    uint32_t pad_;
 };
 
 // Slots of the per-launch 64-bit counter array.
@@ -72,6 +97,14 @@ struct TileArgs {
     uint32_t* wblock;
     uint8_t* wend;
     uint32_t* dbg;
+    // grouped pipeline (kModeCut)
+    uint32_t* rec_key;
+    unsigned long long* rec_val;
+    unsigned long long* rec_count;
+    uint64_t rec_cap;
+    unsigned long long* bucket_hist;
+    uint32_t bucket_shift;
+    uint32_t pad3_;
 };
 
 // Kernel launches; each counts itself in the library-wide launch counter.
@@ -88,6 +121,16 @@ void launch_plain_query(int mode, const TileArgs& a, cudaStream_t st);
 void launch_counter_hist(const void* table, uint64_t slots, int bits, unsigned long long* hist, uint32_t dense,
                          unsigned long long* ovf, uint64_t ovf_cap, unsigned long long* ovf_count, cudaStream_t st);
 void launch_fill_u32(uint32_t* p, uint32_t v, uint64_t n, cudaStream_t st);
+// grouped pipeline
+void launch_scatter(const uint32_t* rec_key, const unsigned long long* rec_val, const unsigned long long* rec_count,
+                    uint64_t rec_cap, uint32_t bucket_shift, unsigned long long* cursor, unsigned long long* sorted,
+                    cudaStream_t st);
+void launch_item_counts(const unsigned long long* bucket_off, uint64_t n_buckets, uint64_t* item_count,
+                        cudaStream_t st);
+void launch_item_write(const unsigned long long* bucket_off, const uint64_t* item_off, uint64_t n_buckets,
+                       uint4* items, cudaStream_t st);
+void launch_apply(int mode, const GroupArgs& a, int block_slots, uint32_t bucket_blocks, int sm_count,
+                  uint64_t max_items, cudaStream_t st);
 
 uint64_t kernel_launch_count();
 void note_launch();

@@ -108,18 +108,50 @@ def test_window_minimizers_match_oracle(scb, oracle_mod, geom):
 
 
 @pytest.mark.parametrize("bits", [8, 16, 32])
-def test_plain_and_fused_strategies_agree(scb, oracle_mod, bits):
+def test_strategies_agree(scb, oracle_mod, bits):
     seqs = _random_batch(5 + bits, 300, 100, 2000)
     res = []
-    for strategy in ("plain", "fused"):
+    for strategy in ("plain", "fused", "grouped"):
         cfg, idx, o, data, offsets, rep, okms = _pair(scb, oracle_mod, 31, 21, 25, 4, 20, 9, bits, seqs, strategy)
         res.append((idx.table(), idx.estimate_batch(data, offsets), idx.query_report(data, offsets),
                     (rep.inserted_kmers, rep.inserted_smers)))
         assert np.array_equal(idx.table(), o.table())
         assert (rep.inserted_kmers, rep.inserted_smers) == okms
-    assert np.array_equal(res[0][0], res[1][0])
-    assert np.array_equal(res[0][1][0], res[1][1][0]) and np.array_equal(res[0][1][1], res[1][1][1])
-    assert res[0][2] == res[1][2]
+    for other in res[1:]:
+        assert np.array_equal(res[0][0], other[0])
+        assert np.array_equal(res[0][1][0], other[1][0]) and np.array_equal(res[0][1][1], other[1][1])
+        assert res[0][2] == other[2]
+
+
+@pytest.mark.parametrize("geom", GEOMETRIES)
+def test_grouped_parity_all_geometries(scb, oracle_mod, geom):
+    k, m, s, h, se, be = geom
+    for bits in (8, 16, 32):
+        seqs = _random_batch(300 + k + bits, 150, 1, 800)
+        cfg, idx, o, data, offsets, rep, okms = _pair(scb, oracle_mod, k, m, s, h, se, be, bits, seqs, "grouped")
+        assert (rep.inserted_kmers, rep.inserted_smers) == okms
+        assert np.array_equal(idx.table(), o.table())
+        q = idx.query_report(data, offsets)
+        oq = o.query_report_arrays(data, offsets)
+        assert (q.valid_kmers, q.positive_estimates, q.estimate_checksum) == (
+            oq.valid_kmers, oq.positive_estimates, oq.estimate_checksum)
+
+
+@pytest.mark.parametrize("bits", [8, 16, 32])
+def test_grouped_hot_buckets_split_and_saturate(scb, oracle_mod, bits):
+    """20000 copies of a few reads put far more than one work item's records in the same
+    buckets: the split items commit through saturating CAS and must still be exact."""
+    rng = np.random.default_rng(4)
+    base = [rng.choice(np.frombuffer(b"ACGT", np.uint8), 150).tobytes() for _ in range(3)]
+    seqs = [base[i % 3] for i in range(20000)] + _random_batch(8, 50, 100, 300)
+    for strategy in ("grouped", "fused"):
+        cfg, idx, o, data, offsets, rep, okms = _pair(scb, oracle_mod, 31, 21, 25, 4, 20, 9, bits, seqs, strategy)
+        assert (rep.inserted_kmers, rep.inserted_smers) == okms
+        assert np.array_equal(idx.table(), o.table())
+        q = idx.query_report(data, offsets)
+        oq = o.query_report_arrays(data, offsets)
+        assert (q.valid_kmers, q.positive_estimates, q.estimate_checksum) == (
+            oq.valid_kmers, oq.positive_estimates, oq.estimate_checksum)
 
 
 def test_save_matches_oracle_bytes_and_roundtrips(scb, oracle_mod):
@@ -220,7 +252,7 @@ def test_workload_medium_parity(scb, oracle_mod):
 
     data, offsets = workloads.short_reads(genome_len=200_000, n_reads=20_000, read_len=150, seed=1,
                                           sub_rate=0.005, n_rate=0.01)
-    for strategy in ("plain", "fused"):
+    for strategy in ("plain", "fused", "grouped"):
         cfg = _cfg(scb, 31, 21, 25, 4, 24, 9, 16)
         b = scb.SuperCountingBloomBuilder(cfg)
         from scbf_b200 import api
@@ -259,7 +291,8 @@ def test_build_and_stream_query_matches_separate_calls(scb, oracle_mod):
     assert (km.value, sm.value) == (okm, osm)
     assert (rep.valid_kmers, rep.positive_estimates, rep.estimate_checksum) == (
         oq.valid_kmers, oq.positive_estimates, oq.estimate_checksum)
-    res = o.port_build_and_stream_query(data, offsets, threads=4)
+    fresh = oracle_mod.OracleFilter(oracle_mod.make_config(31, 21, 25, 4, 16, 22, 9))
+    res = fresh.port_build_and_stream_query(data, offsets, threads=4)
     assert res["report"].estimate_checksum == rep.estimate_checksum
 
 
