@@ -137,6 +137,17 @@ scb_status scb_query_report(scb_ctx* ctx, const uint8_t* seqs, const uint64_t* o
 scb_status scb_query_report_device(scb_ctx* ctx, const uint8_t* d_seqs, const uint64_t* d_offsets,
                                    uint64_t n_seqs, uint64_t n_bytes, void* stream, scb_report* report);
 
+/* No counterpart in the reference.  scb_query_report_device without any device allocation, for
+ * callers that cannot allocate while they run: code inside a CUDA stream capture, real-time
+ * serving threads that keep the allocator out of the request path, hosts that give the library a
+ * fixed memory budget.  Its scratch is one static device array of about 16 MiB that every GPU
+ * loading this library holds until exit; batches are limited to 32 MiB of sequence bytes (larger
+ * ones fail with SCB_ERR_INTERNAL_STATE).  The first call on a device looks up the array's
+ * address; make that first call before any stream capture.  All calls share the array (each
+ * clears what it reads), so calls whose GPU work overlaps race: serialise them. */
+scb_status scb_query_report_device_noalloc(scb_ctx* ctx, const uint8_t* d_seqs, const uint64_t* d_offsets,
+                                           uint64_t n_seqs, uint64_t n_bytes, void* stream, scb_report* report);
+
 /* stream_estimates_from_fastx (src/fastx.rs:107-131, 172-204, 206-253, 310-369) on in-memory
  * records: builds from the records, freezes, then stream-queries the same records.  The
  * records are copied to the device once and kept resident between the two passes. */

@@ -101,6 +101,8 @@ def load(path: str | None = None):
         "scb_set_timing": (C.c_int, [ctxp, C.c_int]),
         "scb_get_timings": (C.c_int, [ctxp, C.POINTER(ScbTimings)]),
         "scb_reset": (C.c_int, [ctxp]),
+        "scb_query_report_device_noalloc": (C.c_int, [ctxp, vp, vp, C.c_uint64, C.c_uint64, vp,
+                                                      C.POINTER(ScbReport)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

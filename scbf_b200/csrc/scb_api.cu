@@ -1202,3 +1202,113 @@ scb_status scb_load(const char* path, scb_ctx** out) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------
+// Allocation-free query report.
+//
+// For callers that must not allocate device memory while they run: code inside a CUDA stream
+// capture (cudaMalloc is not a stream operation and breaks the capture), real-time serving
+// threads that keep allocator latency and fragmentation out of the request path, and hosts that
+// hand this library a fixed memory budget at start-up.  The per-call scratch of the fused
+// report query (2-bit codes, ACGT and sequence-start bitmaps, counters, the tile work counter)
+// lives in one file-scope device array instead of buffers allocated per call.
+//
+// Limits: batches of at most kNoallocMaxBytes sequence bytes.  The array takes
+// kNoallocScratchBytes on every GPU that loads this library, until the process exits.  All calls
+// share it: the call clears what must start at zero, and two calls whose work overlaps on the
+// GPU (different streams or threads) race on it, so such callers serialise their calls.
+// ---------------------------------------------------------------------------------------
+namespace {
+
+constexpr uint64_t kNoallocMaxBytes = 32ull << 20;  // 32 MiB of sequence bytes per call
+constexpr uint64_t kNoallocGroups = kNoallocMaxBytes / 32;
+constexpr uint64_t kNoallocCodesBytes = (2 * kNoallocGroups + kPadWords) * 4;
+constexpr uint64_t kNoallocBitsBytes = (kNoallocGroups + kPadWords) * 4;
+constexpr uint64_t kNoallocCodesOff = 256;  // counters (16 x u64) and the tile counter come first
+constexpr uint64_t kNoallocValidOff = kNoallocCodesOff + ((kNoallocCodesBytes + 255) / 256) * 256;
+constexpr uint64_t kNoallocStartOff = kNoallocValidOff + ((kNoallocBitsBytes + 255) / 256) * 256;
+constexpr uint64_t kNoallocScratchBytes = kNoallocStartOff + ((kNoallocBitsBytes + 255) / 256) * 256;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocScratchBytes];
+
+// Device address of g_noalloc_scratch, looked up once per device with that device current.
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[64] = {nullptr};
+
+scb_status noalloc_scratch(int device, unsigned char** out) {
+    if (device < 0 || device >= 64) return fail_kind(SCB_ERR_INTERNAL_STATE, "device index out of range");
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_addr[device]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            return fail_kind(SCB_ERR_INTERNAL_STATE,
+                             std::string("cudaGetSymbolAddress of the static scratch failed: ") + cudaGetErrorString(e));
+        }
+        g_noalloc_addr[device] = p;
+    }
+    *out = static_cast<unsigned char*>(g_noalloc_addr[device]);
+    return SCB_OK;
+}
+
+}  // namespace
+
+extern "C" scb_status scb_query_report_device_noalloc(scb_ctx* ctx, const uint8_t* d_seqs, const uint64_t* d_offsets,
+                                                      uint64_t n_seqs, uint64_t n_bytes, void* stream,
+                                                      scb_report* report) {
+    SCB_TRY(need_frozen(ctx));
+    if (!report) return fail_kind(SCB_ERR_INTERNAL_STATE, "null report");
+    if (n_bytes > kNoallocMaxBytes) {
+        return fail_kind(SCB_ERR_INTERNAL_STATE, "scb_query_report_device_noalloc takes at most " +
+                                                     std::to_string(kNoallocMaxBytes) + " sequence bytes per call, got " +
+                                                     std::to_string(n_bytes));
+    }
+    CtxLock lk(ctx);
+    unsigned char* base = nullptr;
+    SCB_TRY(noalloc_scratch(ctx->device, &base));
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    const uint64_t groups = (n_bytes + 31) / 32;
+    unsigned long long* cnt = reinterpret_cast<unsigned long long*>(base);
+    unsigned int* tiles = reinterpret_cast<unsigned int*>(base + kCntSlots * 8);
+    uint32_t* codes = reinterpret_cast<uint32_t*>(base + kNoallocCodesOff);
+    uint32_t* valid = reinterpret_cast<uint32_t*>(base + kNoallocValidOff);
+    uint32_t* seqstart = reinterpret_cast<uint32_t*>(base + kNoallocStartOff);
+    // the array keeps the previous call's contents: clear everything this call reads
+    SCB_CUDA(cudaMemsetAsync(base, 0, kNoallocCodesOff, st));
+    SCB_CUDA(cudaMemsetAsync(codes, 0, (2 * groups + kPadWords) * 4, st));
+    SCB_CUDA(cudaMemsetAsync(valid, 0, (groups + kPadWords) * 4, st));
+    SCB_CUDA(cudaMemsetAsync(seqstart, 0, (groups + kPadWords) * 4, st));
+    if (n_bytes) launch_pack(d_seqs, n_bytes, codes, valid, st);
+    launch_seqstart(d_offsets, n_seqs, n_bytes, seqstart, st);
+    launch_seq_windows(d_offsets, n_seqs, ctx->g.k, cnt, nullptr, st);
+    TileArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.g = ctx->g;
+    a.codes = codes;
+    a.valid = valid;
+    a.seqstart = seqstart;
+    a.n_bytes = n_bytes;
+    a.n_code_words = 2 * groups;
+    a.n_bit_words = groups;
+    a.n_tiles = (uint32_t)((n_bytes + kTileWindows - 1) / kTileWindows);
+    a.table = ctx->table;
+    a.status = ctx->status;
+    a.cnt = cnt;
+    a.tile_counter = tiles;
+    a.offsets = d_offsets;
+    a.n_seqs = n_seqs;
+    if (a.n_tiles) launch_tiles(kModeReport, a, tile_grid(kModeReport, ctx->g.bits, ctx->sm_count, a.n_tiles), st);
+    SCB_CUDA(cudaGetLastError());
+    unsigned long long c[kCntSlots];
+    uint32_t status = 0;
+    SCB_CUDA(cudaMemcpyAsync(c, cnt, kCntSlots * 8, cudaMemcpyDeviceToHost, st));
+    SCB_CUDA(cudaMemcpyAsync(&status, ctx->status, 4, cudaMemcpyDeviceToHost, st));
+    SCB_CUDA(cudaStreamSynchronize(st));
+    if (status) return fail_kind(SCB_ERR_INTERNAL_STATE, "device status word 0x" + std::to_string(status));
+    report->records_processed = c[kCntRecords];
+    report->total_windows = c[kCntTotalWindows];
+    report->valid_kmers = c[kCntValid];
+    report->positive_estimates = c[kCntPositive];
+    report->estimate_checksum = c[kCntChecksum];
+    return SCB_OK;
+}
