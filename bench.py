@@ -53,6 +53,8 @@ def parse():
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-mixed", action="store_true", help="skip the mixed-length (config 4) comparison")
+    p.add_argument("--no-serve", action="store_true", help="skip the serving (config 5) measurement")
     p.add_argument("--profile-case", choices=["plain", "fused", "grouped"], default=None,
                    help="run one insert + query of a small case (for ncu) and exit")
     return p.parse_args()
@@ -256,12 +258,10 @@ def run_ours(args, dist: Dist):
     rep = _lib.ScbReport()
 
     def step():
+        # stream_estimates_from_fastx on resident reads: clear, build, freeze, stream-query
         check(L.scb_reset(h))
-        check(L.scb_insert_batch_device(h, d_data.data_ptr(), d_off.data_ptr(), n_seqs, n_bytes, sp, C.byref(km),
-                                        C.byref(sm)))
-        check(L.scb_freeze(h))
-        check(L.scb_query_report_device(h, d_data.data_ptr(), d_off.data_ptr(), n_seqs, n_bytes, sp,
-                                        C.byref(rep)))
+        check(L.scb_build_and_stream_query_device(h, d_data.data_ptr(), d_off.data_ptr(), n_seqs, n_bytes, sp,
+                                                  C.byref(km), C.byref(sm), C.byref(rep)))
 
     def timed(strategy: str, steps: int) -> tuple[float, dict]:
         sid = STRATEGY_IDS[strategy]
@@ -290,7 +290,6 @@ def run_ours(args, dist: Dist):
         info = {"clocks": clk, "launches": L.scb_kernel_launches() - launches0}
         for f in ("pack_ms", "insert_ms", "query_ms", "cut_ms", "bucket_ms", "apply_insert_ms", "apply_query_ms"):
             info[f] = getattr(t, f) / steps
-        info["cut_ms"] /= 2  # one cut per insert and one per query
         info["report"] = (rep.valid_kmers, rep.positive_estimates, rep.estimate_checksum)
         return dist.max(ms), info
 
@@ -371,6 +370,14 @@ def run_ours(args, dist: Dist):
                 "sectors_per_superkmer": st.sectors / max(st.super_kmers, 1),
                 "super_kmers": st.super_kmers, "smers": st.smers, "touched_blocks": touched}
 
+    del d_data, d_off
+    serving = None
+    if not args.no_serve:
+        check(L.scb_set_strategy(h, 0, 0))
+        serving = run_serving(ctx, args, dist.rank)
+    ctx.close()
+    mixed = None if args.no_mixed else run_mixed(args, dist)
+
     cpu = None
     if not args.no_cpu and dist.rank == 0 and dist.world == 1:
         from oracle import oracle
@@ -402,12 +409,192 @@ def run_ours(args, dist: Dist):
             "query_kmers_per_s": kmers / (info["query_ms"] / 1e3),
             "stage_ms": {k_: info[k_] for k_ in ("pack_ms", "insert_ms", "query_ms", "cut_ms", "bucket_ms",
                                                  "apply_insert_ms", "apply_query_ms")},
-            "plain": plain, "strategies": strategies, "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
+            "plain": plain, "strategies": strategies, "mixed": mixed, "serve": serving, "e2e": e2e,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
             "clocks": info["clocks"], "gpu_launches": info["launches"],
         }
         print(json.dumps(line), flush=True)
-    del d_data, d_off
+
+
+def run_serving(ctx, args, rank: int) -> dict:
+    """Config-5 shape on the resident config-2 index: requests of sequences, half drawn from the
+    indexed genome (1% errors) and half uniform random, arriving as a Poisson process; the
+    server batches them as they arrive.  Two streams: fixed-size requests of about 1 M k-mers
+    (the p99 < 10 ms target) and the mixed-size stream (1-10^5 sequences of 100 bp-50 kbp, each
+    request truncated at 4 Mbp so the pool is generated in seconds)."""
+    import threading
+
+    from scbf_b200 import _lib, workloads
+
+    L = _lib.load()
+    genome = workloads.random_genome(int(100_000_000 * args.scale), seed=1 + rank)
+    rng = np.random.default_rng(17)
+
+    def pool_fixed(count):
+        reqs = []
+        for i in range(count):
+            d, o = workloads.random_sequences(40, 25_000, 25_001, seed=1000 + i, genome=genome)
+            reqs.append((d, o))
+        return reqs
+
+    def pool_mixed(count, cap_bytes=4_000_000):
+        reqs = []
+        for i in range(count):
+            n = int(np.exp(rng.uniform(0, np.log(1e5))))
+            d, o = workloads.random_sequences(min(n, 4000), 100, 50_000, seed=2000 + i, genome=genome)
+            keep = int(np.searchsorted(o, cap_bytes, side="right")) - 1
+            keep = max(1, min(keep, len(o) - 1))
+            reqs.append((d[: int(o[keep])], o[: keep + 1].copy()))
+        return reqs
+
+    def stream(reqs, rate, seconds, max_batch_bytes):
+        cfg = _lib.ScbServerConfig(16 << 30, max_batch_bytes, 0, 4, 0)
+        srv = C.c_void_p(0)
+        if L.scb_server_create(ctx.h, C.byref(cfg), C.byref(srv)) != 0:
+            raise RuntimeError(_lib.last_error())
+        outs = []
+        for d, o in reqs:
+            nw = int(L.scb_count_windows(ctx.h, o.ctypes.data, len(o) - 1))
+            outs.append((np.empty(max(nw, 1), np.uint64), np.empty(max(nw, 1), np.uint8), nw))
+        # warm-up: every template once
+        for (d, o), (ob, vb, _) in zip(reqs, outs):
+            t = C.c_uint64(0)
+            L.scb_server_submit(srv, d.ctypes.data, o.ctypes.data, len(o) - 1, ob.ctypes.data, vb.ctypes.data,
+                                C.byref(t))
+            L.scb_server_wait(srv, t.value, None)
+        L.scb_server_reset_stats(srv)
+        n_req = max(1, int(rate * seconds))
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, n_req))
+        pick = rng.integers(0, len(reqs), n_req)
+        tickets = []
+        lock = threading.Lock()
+        done = threading.Event()
+
+        def waiter():
+            i = 0
+            while True:
+                with lock:
+                    have = i < len(tickets)
+                    t = tickets[i] if have else None
+                if have:
+                    L.scb_server_wait(srv, t, None)
+                    i += 1
+                    if i == n_req:
+                        break
+                elif done.is_set() and i >= len(tickets):
+                    break
+                else:
+                    time.sleep(0.0002)
+
+        wt = threading.Thread(target=waiter)
+        wt.start()
+        t0 = time.perf_counter()
+        for a, j in zip(arrivals, pick):
+            delay = t0 + a - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            d, o = reqs[j]
+            ob, vb, _ = outs[j]  # requests of one template share output buffers (results not read)
+            t = C.c_uint64(0)
+            L.scb_server_submit(srv, d.ctypes.data, o.ctypes.data, len(o) - 1, ob.ctypes.data, vb.ctypes.data,
+                                C.byref(t))
+            with lock:
+                tickets.append(t.value)
+        done.set()
+        wt.join()
+        s = _lib.ScbServerSummary()
+        L.scb_server_get_summary(srv, C.byref(s))
+        L.scb_server_destroy(srv)
+        return {"rate_req_s": rate, "requests": s.requests, "p50_ms": s.p50_ms, "p99_ms": s.p99_ms,
+                "mean_ms": s.mean_ms, "max_ms": s.max_ms, "kmers_per_s": s.windows / s.span_s if s.span_s else None,
+                "batches": s.batches, "slots": s.slots,
+                "mean_kmers_per_request": float(np.mean([outs[j][2] for j in pick]))}
+
+    fixed = stream(pool_fixed(16), rate=300.0, seconds=3.0, max_batch_bytes=16 << 20)
+    mixed = stream(pool_mixed(48), rate=100.0, seconds=3.0, max_batch_bytes=32 << 20)
+    return {"index": "config-2 frozen index, resident", "one_mkmer_requests": fixed, "mixed_requests": mixed}
+
+
+MIXED_WORKLOAD = ("mixed lengths: 200 Mbp uniform genome at 15x; 70% of bases from 150 bp reads (1% "
+                  "substitutions), 30% from log-normal long reads (median 10 kbp, 1-100 kbp, 5% errors, "
+                  "sub:ins:del = 2:1:1); default geometry with 2^31 16-bit slots (4 GiB)")
+
+
+def run_mixed(args, dist: Dist) -> dict:
+    """Config-4 shape: insert then query every read of an uneven-length workload, in device
+    batches of at most 1.6 GB, per strategy.  Returns k-mers/s per strategy."""
+    import torch
+
+    from scbf_b200 import _lib, api, workloads
+
+    L = _lib.load()
+    data, offsets = workloads.config4(seed=7 + dist.rank, scale=args.scale)
+    # split into batches of whole reads of at most 1.6 GB
+    cuts = [0]
+    limit = 1_600_000_000
+    while int(offsets[-1]) - int(offsets[cuts[-1]]) > limit:
+        cuts.append(int(np.searchsorted(offsets, offsets[cuts[-1]] + limit, side="right")) - 1)
+    cuts.append(len(offsets) - 1)
+    batches = []
+    for a, b in zip(cuts[:-1], cuts[1:]):
+        o = (offsets[a:b + 1] - offsets[a]).astype(np.uint64)
+        d = data[int(offsets[a]):int(offsets[b])]
+        batches.append((torch.from_numpy(d).to("cuda"), torch.from_numpy(o.view(np.int64)).to("cuda"), b - a,
+                        int(o[-1])))
+    del data
+    cfg = api.SuperCountingBloomConfig(k=GEOM["k"], m=GEOM["m"], s=GEOM["s"], n_hashes=GEOM["n_hashes"],
+                                       counter_bits=api.CounterBits(16), counter_slots_exponent=31,
+                                       block_slots_exponent=GEOM["block_slots_exponent"], threads=1, queue=4096)
+    ctx = api._create(cfg)
+    h = ctx.h
+    km, sm = C.c_uint64(0), C.c_uint64(0)
+    rep = _lib.ScbReport()
+
+    def check(st):
+        if st != 0:
+            raise RuntimeError(_lib.last_error())
+
+    def step():
+        check(L.scb_reset(h))
+        total = 0
+        for d, o, n, nb in batches:
+            check(L.scb_insert_batch_device(h, d.data_ptr(), o.data_ptr(), n, nb, None, C.byref(km), C.byref(sm)))
+            total += km.value
+        check(L.scb_freeze(h))
+        chk = 0
+        for d, o, n, nb in batches:
+            check(L.scb_query_report_device(h, d.data_ptr(), o.data_ptr(), n, nb, None, C.byref(rep)))
+            chk = (chk + rep.estimate_checksum) % (1 << 64)
+        return total, chk
+
+    out = {"workload": MIXED_WORKLOAD + (f" (genome scale {args.scale})" if args.scale != 1.0 else ""),
+           "reads": int(len(offsets) - 1), "bytes": int(offsets[-1]), "batches": len(batches)}
+    ref = None
+    for name in ("plain", "fused", "grouped", "auto"):
+        sid = STRATEGY_IDS[name]
+        check(L.scb_set_strategy(h, sid, sid))
+        steps = max(1, args.steps // 2)
+        for _ in range(min(args.warmup, 2)):
+            res = step()
+        torch.cuda.synchronize()
+        dist.barrier()
+        t0 = time.perf_counter()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        for _ in range(steps):
+            res = step()
+        ev1.record()
+        torch.cuda.synchronize()
+        ms = dist.max(ev0.elapsed_time(ev1))
+        if ref is None:
+            ref = res
+        assert res == ref, (name, res, ref)
+        out[name] = dist.sum(float(res[0])) * steps / (ms / 1e3)
+    out["kmers_per_step"] = ref[0]
+    out["batched_over_plain"] = out["auto"] / out["plain"]
     ctx.close()
+    return out
 
 
 def run_profile_case(args):
@@ -431,11 +618,8 @@ def run_profile_case(args):
     km, sm = C.c_uint64(0), C.c_uint64(0)
     rep = _lib.ScbReport()
     n = len(offsets) - 1
-    assert L.scb_insert_batch_device(ctx.h, d_data.data_ptr(), d_off.data_ptr(), n, int(offsets[-1]), None,
-                                     C.byref(km), C.byref(sm)) == 0, _lib.last_error()
-    assert L.scb_freeze(ctx.h) == 0
-    assert L.scb_query_report_device(ctx.h, d_data.data_ptr(), d_off.data_ptr(), n, int(offsets[-1]), None,
-                                     C.byref(rep)) == 0, _lib.last_error()
+    assert L.scb_build_and_stream_query_device(ctx.h, d_data.data_ptr(), d_off.data_ptr(), n, int(offsets[-1]),
+                                               None, C.byref(km), C.byref(sm), C.byref(rep)) == 0, _lib.last_error()
     torch.cuda.synchronize()
     print(json.dumps({"profile_case": args.profile_case, "kmers": km.value, "smers": sm.value,
                       "checksum": rep.estimate_checksum}), flush=True)

@@ -151,6 +151,10 @@ scb_status scb_query_report_device_noalloc(scb_ctx* ctx, const uint8_t* d_seqs, 
 /* stream_estimates_from_fastx (src/fastx.rs:107-131, 172-204, 206-253, 310-369) on in-memory
  * records: builds from the records, freezes, then stream-queries the same records.  The
  * records are copied to the device once and kept resident between the two passes. */
+scb_status scb_build_and_stream_query_device(scb_ctx* ctx, const uint8_t* d_seqs, const uint64_t* d_offsets,
+                                             uint64_t n_seqs, uint64_t n_bytes, void* stream,
+                                             uint64_t* inserted_kmers, uint64_t* inserted_smers,
+                                             scb_report* report);
 scb_status scb_build_and_stream_query(scb_ctx* ctx, const uint8_t* seqs, const uint64_t* offsets,
                                       uint64_t n_seqs, uint64_t* inserted_kmers, uint64_t* inserted_smers,
                                       scb_report* report);
@@ -206,6 +210,50 @@ typedef struct scb_timings {
 } scb_timings;
 scb_status scb_set_timing(scb_ctx* ctx, int enable); /* enabling also clears the totals */
 scb_status scb_get_timings(const scb_ctx* ctx, scb_timings* out);
+
+/* ---------------------------------------------------------------------------------------
+ * Serving: a request loop over a frozen, device-resident index (no counterpart in the
+ * reference, whose queries run per call; this batches SuperCountingBloomIndex::
+ * estimate_sequence_abundances requests, src/api.rs:250-262, as they arrive).
+ * Requests are split into pieces of whole sequences; pending pieces are packed into batches
+ * of at most max_batch_bytes / max_batch_seqs and run on one of several slots (streams with
+ * their own device buffers) as soon as a slot is free, so batches overlap on the GPU.  The
+ * number of slots is min(max_inflight, memory_budget_bytes / bytes of one slot): the budget
+ * admits work.  Results are bit-identical to scb_query_batch on the same request.
+ * --------------------------------------------------------------------------------------- */
+typedef struct scb_server scb_server;
+typedef struct scb_server_config {
+    uint64_t memory_budget_bytes; /* device bytes for in-flight batches (0: max_inflight slots) */
+    uint64_t max_batch_bytes;     /* sequence bytes per batch (default 64 MiB, at most 1 GiB) */
+    uint64_t max_batch_seqs;      /* sequences per batch (default max_batch_bytes / 64) */
+    uint32_t max_inflight;        /* batches on the GPU at once (default 4) */
+    uint32_t reserved;
+} scb_server_config;
+typedef struct scb_request_stats {
+    double queue_ms;   /* submit -> first piece launched */
+    double service_ms; /* first piece launched -> results written */
+    double total_ms;   /* submit -> results written */
+    uint64_t windows;
+} scb_request_stats;
+typedef struct scb_server_summary {
+    uint64_t requests; /* completed since the last reset */
+    uint64_t windows;
+    uint64_t batches;
+    double p50_ms, p99_ms, mean_ms, max_ms; /* submit -> results written */
+    double span_s;                          /* first submit -> last completion */
+    uint32_t slots;
+    uint32_t reserved;
+} scb_server_summary;
+scb_status scb_server_create(scb_ctx* index, const scb_server_config* cfg, scb_server** out);
+/* Queues a request; host buffers stay owned by the caller and must stay valid until
+ * scb_server_wait(ticket) returns.  Outputs are laid out as for scb_query_batch. */
+scb_status scb_server_submit(scb_server* s, const uint8_t* seqs, const uint64_t* offsets, uint64_t n_seqs,
+                             uint64_t* abundances, uint8_t* valid, uint64_t* ticket);
+scb_status scb_server_wait(scb_server* s, uint64_t ticket, scb_request_stats* stats);
+scb_status scb_server_get_summary(scb_server* s, scb_server_summary* out);
+scb_status scb_server_reset_stats(scb_server* s);
+/* Drains in-flight batches, then frees the server (not the index). */
+void scb_server_destroy(scb_server* s);
 
 /* Clears the counter table and the insert totals and makes the context a builder again
  * (SuperCountingBloomBuilder::new on the existing allocation). */

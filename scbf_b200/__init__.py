@@ -23,6 +23,7 @@ from .api import (  # noqa: F401
     SuperCountingBloomError,
     SuperCountingBloomIndex,
     SuperCountingBloomReport,
+    SuperCountingBloomServer,
     SuperCountingBloomStats,
     WorkerPanic,
     estimate_spectrum_from_fastx,

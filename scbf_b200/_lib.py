@@ -45,6 +45,22 @@ class ScbTimings(C.Structure):
                 ("apply_insert_ms", C.c_double), ("apply_query_ms", C.c_double)]
 
 
+class ScbServerConfig(C.Structure):
+    _fields_ = [("memory_budget_bytes", C.c_uint64), ("max_batch_bytes", C.c_uint64),
+                ("max_batch_seqs", C.c_uint64), ("max_inflight", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class ScbRequestStats(C.Structure):
+    _fields_ = [("queue_ms", C.c_double), ("service_ms", C.c_double), ("total_ms", C.c_double),
+                ("windows", C.c_uint64)]
+
+
+class ScbServerSummary(C.Structure):
+    _fields_ = [("requests", C.c_uint64), ("windows", C.c_uint64), ("batches", C.c_uint64),
+                ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("mean_ms", C.c_double), ("max_ms", C.c_double),
+                ("span_s", C.c_double), ("slots", C.c_uint32), ("reserved", C.c_uint32)]
+
+
 _lib = None
 
 
@@ -87,6 +103,8 @@ def load(path: str | None = None):
         "scb_query_report": (C.c_int, [ctxp, vp, vp, C.c_uint64, C.POINTER(ScbReport)]),
         "scb_query_report_device": (C.c_int, [ctxp, vp, vp, C.c_uint64, C.c_uint64, vp, C.POINTER(ScbReport)]),
         "scb_build_and_stream_query": (C.c_int, [ctxp, vp, vp, C.c_uint64, u64p, u64p, C.POINTER(ScbReport)]),
+        "scb_build_and_stream_query_device": (C.c_int, [ctxp, vp, vp, C.c_uint64, C.c_uint64, vp, u64p, u64p,
+                                                        C.POINTER(ScbReport)]),
         "scb_spectrum_distinct": (C.c_int, [ctxp, vp, vp, C.c_uint64, vp, vp, C.c_uint64, u64p, u64p, u64p]),
         "scb_counter_histogram": (C.c_int, [ctxp, vp, vp, C.c_uint64, u64p]),
         "scb_save": (C.c_int, [ctxp, C.c_char_p]),
@@ -103,6 +121,12 @@ def load(path: str | None = None):
         "scb_reset": (C.c_int, [ctxp]),
         "scb_query_report_device_noalloc": (C.c_int, [ctxp, vp, vp, C.c_uint64, C.c_uint64, vp,
                                                       C.POINTER(ScbReport)]),
+        "scb_server_create": (C.c_int, [ctxp, C.POINTER(ScbServerConfig), C.POINTER(vp)]),
+        "scb_server_submit": (C.c_int, [vp, vp, vp, C.c_uint64, vp, vp, u64p]),
+        "scb_server_wait": (C.c_int, [vp, C.c_uint64, C.POINTER(ScbRequestStats)]),
+        "scb_server_get_summary": (C.c_int, [vp, C.POINTER(ScbServerSummary)]),
+        "scb_server_reset_stats": (C.c_int, [vp]),
+        "scb_server_destroy": (None, [vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -634,3 +634,69 @@ def write_spectrum(spectrum, output=None) -> None:
             fh.write(text)
     except OSError as err:
         raise Io(f"I/O error for '{output}': {err}") from err
+
+
+# ---------------------------------------------------------------------------------------
+# Serving (continuous batching over a device-resident frozen index)
+# ---------------------------------------------------------------------------------------
+@dataclass
+class RequestStats:
+    queue_ms: float
+    service_ms: float
+    total_ms: float
+    windows: int
+
+
+class SuperCountingBloomServer:
+    """Request loop over a frozen index: submit() queues a request of sequences and returns a
+    ticket immediately; wait(ticket) returns its per-window abundances and validity flags (the
+    layout of SuperCountingBloomIndex.estimate_batch).  Requests arriving while others run share
+    batches and overlap on the GPU; the device-memory budget bounds the batches in flight."""
+
+    def __init__(self, index: "SuperCountingBloomIndex", memory_budget_bytes: int = 0,
+                 max_batch_bytes: int = 64 << 20, max_batch_seqs: int = 0, max_inflight: int = 4):
+        self.index = index
+        cfg = _lib.ScbServerConfig(memory_budget_bytes, max_batch_bytes, max_batch_seqs, max_inflight, 0)
+        out = C.c_void_p(0)
+        _check(_lib.load().scb_server_create(index._ctx.h, C.byref(cfg), C.byref(out)))
+        self.h = out
+        self._live: dict[int, tuple] = {}
+
+    def submit(self, data: np.ndarray, offsets: np.ndarray) -> int:
+        data, offsets = _as_batch(data, offsets)
+        n = len(offsets) - 1
+        nw = int(_lib.load().scb_count_windows(self.index._ctx.h, _ptr(offsets), n))
+        out = np.zeros(max(nw, 1), dtype=np.uint64)
+        valid = np.zeros(max(nw, 1), dtype=np.uint8)
+        t = C.c_uint64(0)
+        _check(_lib.load().scb_server_submit(self.h, _ptr(data), _ptr(offsets), n, _ptr(out), _ptr(valid),
+                                             C.byref(t)))
+        self._live[t.value] = (data, offsets, out, valid, nw)  # keeps the buffers alive
+        return t.value
+
+    def wait(self, ticket: int) -> tuple[np.ndarray, np.ndarray, RequestStats]:
+        st = _lib.ScbRequestStats()
+        rc = _lib.load().scb_server_wait(self.h, ticket, C.byref(st))
+        data, offsets, out, valid, nw = self._live.pop(ticket)
+        _check(rc)
+        return out[:nw], valid[:nw], RequestStats(st.queue_ms, st.service_ms, st.total_ms, st.windows)
+
+    def summary(self) -> dict:
+        s = _lib.ScbServerSummary()
+        _check(_lib.load().scb_server_get_summary(self.h, C.byref(s)))
+        return {"requests": s.requests, "windows": s.windows, "batches": s.batches, "p50_ms": s.p50_ms,
+                "p99_ms": s.p99_ms, "mean_ms": s.mean_ms, "max_ms": s.max_ms, "span_s": s.span_s, "slots": s.slots}
+
+    def reset_stats(self) -> None:
+        _check(_lib.load().scb_server_reset_stats(self.h))
+
+    def close(self) -> None:
+        if self.h and self.h.value:
+            _lib.load().scb_server_destroy(self.h)
+            self.h = C.c_void_p(0)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -11,130 +11,9 @@
 #include <vector>
 
 #include "../../include/scb.h"
-#include "scb_kernels.cuh"
+#include "scb_internal.h"
 
 using namespace scb;
-
-// ---------------------------------------------------------------------------------------
-// Errors
-// ---------------------------------------------------------------------------------------
-namespace {
-
-thread_local std::string g_last_error;
-
-scb_status fail(scb_status st, const std::string& msg) {
-    g_last_error = msg;
-    return st;
-}
-
-const char* kind_prefix(scb_status st) {
-    switch (st) {
-        case SCB_ERR_INVALID_CONFIG: return "invalid config: ";
-        case SCB_ERR_INVALID_INDEX_FORMAT: return "invalid index format: ";
-        case SCB_ERR_INTERNAL_STATE: return "internal state error: ";
-        case SCB_ERR_IO: return "I/O error for ";
-        default: return "";
-    }
-}
-
-scb_status fail_kind(scb_status st, const std::string& msg) { return fail(st, std::string(kind_prefix(st)) + msg); }
-
-#define SCB_CUDA(call)                                                                               \
-    do {                                                                                             \
-        cudaError_t e_ = (call);                                                                     \
-        if (e_ != cudaSuccess) {                                                                     \
-            return fail_kind(SCB_ERR_INTERNAL_STATE, std::string(#call) + ": " + cudaGetErrorString(e_)); \
-        }                                                                                            \
-    } while (0)
-
-#define SCB_TRY(expr)                 \
-    do {                              \
-        scb_status s_ = (expr);       \
-        if (s_ != SCB_OK) return s_;  \
-    } while (0)
-
-// ---------------------------------------------------------------------------------------
-// Device buffers
-// ---------------------------------------------------------------------------------------
-struct DevBuf {
-    void* p = nullptr;
-    size_t cap = 0;
-    ~DevBuf() {
-        if (p) cudaFree(p);
-    }
-    scb_status ensure(size_t bytes) {
-        if (bytes <= cap) return SCB_OK;
-        if (p) {
-            cudaFree(p);
-            p = nullptr;
-            cap = 0;
-        }
-        size_t want = std::max<size_t>(bytes, 256);
-        cudaError_t e = cudaMalloc(&p, want);
-        if (e != cudaSuccess) {
-            p = nullptr;
-            return fail_kind(SCB_ERR_INTERNAL_STATE,
-                             "device allocation of " + std::to_string(want) + " bytes failed: " + cudaGetErrorString(e));
-        }
-        cap = want;
-        return SCB_OK;
-    }
-    template <typename T>
-    T* as() const {
-        return reinterpret_cast<T*>(p);
-    }
-};
-
-// Largest batch the kernels index with 32-bit positions.
-constexpr uint64_t kMaxBatchBytes = (1ull << 31);
-constexpr uint64_t kPadWords = 16;
-
-// Derived per-batch arrays (codes, bitmaps, window offsets, plain-pipeline arrays, counters).
-struct Lane {
-    DevBuf ascii, offsets, codes, valid, seqstart, woff, scan, wblock, wend, cnt, tiles;
-    // grouped pipeline: records, bucket offsets / cursors, work items
-    DevBuf rec_key, rec_val, rec_sorted, bhist, bcursor, icount, items, gscan, rec_count;
-    cudaStream_t stream = nullptr;
-    // stage timing: [0,1] pack, [2,3] main stage (main_kind 1 = insert, 2 = query),
-    // [4,5,6,7] grouped cut start / cut end / apply start / apply end (grouped_kind as main_kind)
-    cudaEvent_t ev[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
-    bool pack_timed = false;
-    int main_kind = 0;
-    int grouped_kind = 0;
-    ~Lane() {
-        for (auto& e : ev) {
-            if (e) cudaEventDestroy(e);
-        }
-        if (stream) cudaStreamDestroy(stream);
-    }
-};
-
-}  // namespace
-
-struct scb_ctx {
-    scb_config cfg{};
-    DevGeom g{};
-    // FrozenFilterLayout (filter.rs:77-116)
-    uint64_t shard_count = 0, subblocks = 0, block_slots = 0, shard_mask = 0, block_slots_mask = 0, nb_blocks = 0,
-             block_mask = 0;
-    uint32_t shard_shift = 0;
-    int device = 0;
-    int sm_count = 148;
-    void* table = nullptr;
-    uint64_t table_bytes = 0;
-    uint32_t* status = nullptr;
-    bool frozen = false;
-    uint64_t inserted_kmers = 0, inserted_smers = 0;
-    scb_strategy insert_strategy = SCB_STRATEGY_AUTO, query_strategy = SCB_STRATEGY_AUTO;
-    Lane lane;
-    bool timing = false;
-    scb_timings times{};
-    std::mutex mu;
-    ~scb_ctx() {
-        if (table) cudaFree(table);
-        if (status) cudaFree(status);
-    }
-};
 
 namespace {
 
@@ -267,6 +146,7 @@ scb_status ensure_lane(scb_ctx* ctx, Lane& L, uint64_t n_bytes, uint64_t n_seqs)
 scb_status prepare_batch(scb_ctx* ctx, Lane& L, const uint8_t* d_ascii, const uint64_t* d_offsets, uint64_t n_seqs,
                          uint64_t n_bytes, cudaStream_t st, TileArgs& a) {
     const uint64_t groups = (n_bytes + 31) / 32;
+    L.gs.valid = false;
     if (ctx->timing) SCB_CUDA(cudaEventRecord(L.ev[0], st));
     SCB_CUDA(cudaMemsetAsync(L.codes.p, 0, (2 * groups + kPadWords) * 4, st));
     SCB_CUDA(cudaMemsetAsync(L.valid.p, 0, (groups + kPadWords) * 4, st));
@@ -340,11 +220,14 @@ scb_status run_materialize(scb_ctx* ctx, Lane& L, TileArgs& a, cudaStream_t st) 
     return run_tiles(ctx, L, kModeMaterialize, a, st);
 }
 
-// Grouped pipeline for one batch: cut into records, bucket them by block, build work items and
-// run the shared-memory apply kernel (insert or report query).
-scb_status run_grouped(scb_ctx* ctx, Lane& L, int mode, TileArgs& a, cudaStream_t st) {
-    if (a.n_tiles == 0) return SCB_OK;
-    uint64_t cap = records_estimate(ctx, a.n_bytes) * 5 / 4 + 65536;
+// Grouped pipeline, first half: cut the batch into super-k-mer records, bucket them by block and
+// build the work items.  The prepared records stay valid for the lane's current batch, so a
+// query of the same reads (build then stream-query) reuses them.
+scb_status grouped_prepare(scb_ctx* ctx, Lane& L, TileArgs& a, cudaStream_t st) {
+    GroupedState& gs = L.gs;
+    gs.valid = false;
+    // records plus the unused tail of each CTA's last reserved chunk of 4096 slots
+    uint64_t cap = records_estimate(ctx, a.n_bytes) * 5 / 4 + (uint64_t)(ctx->sm_count * 16 + 64) * 4096;
     const uint32_t shift = bucket_shift_for(ctx, records_estimate(ctx, a.n_bytes));
     const uint64_t n_buckets = ctx->nb_blocks >> shift;
     SCB_TRY(L.bhist.ensure((n_buckets + 1) * 8));
@@ -375,42 +258,70 @@ scb_status run_grouped(scb_ctx* ctx, Lane& L, int mode, TileArgs& a, cudaStream_
         SCB_CUDA(cudaMemcpyAsync(&produced, L.rec_count.p, 8, cudaMemcpyDeviceToHost, st));
         SCB_CUDA(cudaStreamSynchronize(st));
         if (produced <= cap) break;
-        cap = produced + 1024;  // more super-k-mers than estimated: size exactly and cut again
+        // more record slots than estimated: the count is exact up to the unused chunk tails of
+        // each CTA, so this capacity always suffices for the second cut
+        cap = produced + (uint64_t)(ctx->sm_count * 16 + 64) * 4096;
     }
     if (produced > cap) return fail_kind(SCB_ERR_INTERNAL_STATE, "super-k-mer record overflow");
-    if (produced == 0) return SCB_OK;
-    SCB_TRY(L.rec_sorted.ensure(produced * 8));
-    launch_scan_inplace(reinterpret_cast<uint64_t*>(L.bhist.p), n_buckets + 1, L.gscan.as<uint64_t>(), st);
-    SCB_CUDA(cudaMemcpyAsync(L.bcursor.p, L.bhist.p, (n_buckets + 1) * 8, cudaMemcpyDeviceToDevice, st));
-    launch_scatter(a.rec_key, a.rec_val, a.rec_count, cap, shift, L.bcursor.as<unsigned long long>(),
-                   L.rec_sorted.as<unsigned long long>(), st);
-    launch_item_counts(L.bhist.as<unsigned long long>(), n_buckets, L.icount.as<uint64_t>(), st);
-    launch_scan_inplace(L.icount.as<uint64_t>(), n_buckets + 1, L.gscan.as<uint64_t>(), st);
-    const uint64_t max_items = std::min<uint64_t>(n_buckets, produced) + produced / kItemRecords + 1;
-    SCB_TRY(L.items.ensure(max_items * 16));
-    launch_item_write(L.bhist.as<unsigned long long>(), L.icount.as<uint64_t>(), n_buckets, L.items.as<uint4>(), st);
-    GroupArgs ga;
+    gs.produced = produced;
+    gs.shift = shift;
+    gs.n_buckets = n_buckets;
+    gs.max_items = 0;
+    if (produced) {
+        SCB_TRY(L.rec_sorted.ensure(produced * 8));
+        launch_scan_inplace(reinterpret_cast<uint64_t*>(L.bhist.p), n_buckets + 1, L.gscan.as<uint64_t>(), st);
+        SCB_CUDA(cudaMemcpyAsync(L.bcursor.p, L.bhist.p, (n_buckets + 1) * 8, cudaMemcpyDeviceToDevice, st));
+        launch_scatter(a.rec_key, a.rec_val, a.rec_count, cap, shift, L.bcursor.as<unsigned long long>(),
+                       L.rec_sorted.as<unsigned long long>(), st);
+        launch_item_counts(L.bhist.as<unsigned long long>(), n_buckets, L.icount.as<uint64_t>(), st);
+        launch_scan_inplace(L.icount.as<uint64_t>(), n_buckets + 1, L.gscan.as<uint64_t>(), st);
+        gs.max_items = std::min<uint64_t>(n_buckets, produced) + produced / kItemRecords + 1;
+        SCB_TRY(L.items.ensure(gs.max_items * 16));
+        launch_item_write(L.bhist.as<unsigned long long>(), L.icount.as<uint64_t>(), n_buckets,
+                          L.items.as<uint4>(), st);
+    }
+    GroupArgs& ga = gs.ga;
     std::memset(&ga, 0, sizeof(ga));
     ga.g = ctx->g;
     ga.codes = a.codes;
     ga.n_code_words = a.n_code_words;
     ga.table = ctx->table;
     ga.status = ctx->status;
-    ga.cnt = a.cnt;
     ga.recs = L.rec_sorted.as<unsigned long long>();
     ga.items = L.items.as<uint4>();
     ga.n_items = reinterpret_cast<const unsigned long long*>(L.icount.as<uint64_t>() + n_buckets);
     ga.work_counter = L.tiles.as<unsigned int>() + 1;
     ga.bucket_shift = shift;
+    if (ctx->timing) {
+        SCB_CUDA(cudaEventRecord(L.ev[6], st));
+        L.cut_timed = true;
+    }
+    gs.valid = true;
+    return SCB_OK;
+}
+
+// Grouped pipeline, second half: the shared-memory apply kernel over the prepared work items.
+scb_status grouped_apply(scb_ctx* ctx, Lane& L, int mode, unsigned long long* cnt, cudaStream_t st) {
+    GroupedState& gs = L.gs;
+    if (!gs.valid) return fail_kind(SCB_ERR_INTERNAL_STATE, "no prepared super-k-mer records");
+    if (gs.produced == 0) return SCB_OK;
+    GroupArgs ga = gs.ga;
+    ga.cnt = cnt;
     SCB_CUDA(cudaMemsetAsync(ga.work_counter, 0, 4, st));
-    if (ctx->timing) SCB_CUDA(cudaEventRecord(L.ev[6], st));
-    launch_apply(mode, ga, (int)ctx->cfg.block_slots_exponent, 1u << shift, ctx->sm_count, max_items, st);
+    if (ctx->timing) SCB_CUDA(cudaEventRecord(L.ev[7], st));
+    launch_apply(mode, ga, (int)ctx->cfg.block_slots_exponent, 1u << gs.shift, ctx->sm_count, gs.max_items, st);
     SCB_CUDA(cudaGetLastError());
     if (ctx->timing) {
-        SCB_CUDA(cudaEventRecord(L.ev[7], st));
+        SCB_CUDA(cudaEventRecord(L.ev[8], st));
         L.grouped_kind = mode == kModeInsert ? 1 : 2;
     }
     return SCB_OK;
+}
+
+scb_status run_grouped(scb_ctx* ctx, Lane& L, int mode, TileArgs& a, cudaStream_t st) {
+    if (a.n_tiles == 0) return SCB_OK;
+    SCB_TRY(grouped_prepare(ctx, L, a, st));
+    return grouped_apply(ctx, L, mode, a.cnt, st);
 }
 
 scb_status insert_stage(scb_ctx* ctx, Lane& L, TileArgs& a, cudaStream_t st) {
@@ -427,7 +338,11 @@ scb_status insert_stage(scb_ctx* ctx, Lane& L, TileArgs& a, cudaStream_t st) {
 
 scb_status query_stage(scb_ctx* ctx, Lane& L, int mode, TileArgs& a, cudaStream_t st) {
     const scb_strategy s = resolve(ctx, ctx->query_strategy, a.n_bytes);
-    if (s == SCB_STRATEGY_GROUPED && mode == kModeReport) return run_grouped(ctx, L, kModeReport, a, st);
+    if (s == SCB_STRATEGY_GROUPED && mode == kModeReport) {
+        // the lane's batch was already cut by a grouped insert of the same reads: reuse its records
+        if (L.gs.valid) return grouped_apply(ctx, L, kModeReport, a.cnt, st);
+        return run_grouped(ctx, L, kModeReport, a, st);
+    }
     if (s == SCB_STRATEGY_PLAIN && (mode == kModeReport || mode == kModeAbund)) {
         SCB_TRY(run_materialize(ctx, L, a, st));
         launch_plain_query(mode, a, st);
@@ -469,13 +384,14 @@ scb_status read_counters(scb_ctx* ctx, Lane& L, cudaStream_t st, unsigned long l
         if (L.main_kind && cudaEventElapsedTime(&ms, L.ev[2], L.ev[3]) == cudaSuccess) {
             (L.main_kind == 1 ? ctx->times.insert_ms : ctx->times.query_ms) += ms;
         }
-        if (L.grouped_kind) {
+        if (L.cut_timed) {
             if (cudaEventElapsedTime(&ms, L.ev[4], L.ev[5]) == cudaSuccess) ctx->times.cut_ms += ms;
             if (cudaEventElapsedTime(&ms, L.ev[5], L.ev[6]) == cudaSuccess) ctx->times.bucket_ms += ms;
-            if (cudaEventElapsedTime(&ms, L.ev[6], L.ev[7]) == cudaSuccess) {
-                (L.grouped_kind == 1 ? ctx->times.apply_insert_ms : ctx->times.apply_query_ms) += ms;
-            }
         }
+        if (L.grouped_kind && cudaEventElapsedTime(&ms, L.ev[7], L.ev[8]) == cudaSuccess) {
+            (L.grouped_kind == 1 ? ctx->times.apply_insert_ms : ctx->times.apply_query_ms) += ms;
+        }
+        L.cut_timed = false;
         if (L.pack_timed || L.main_kind) ctx->times.batches++;
         L.pack_timed = false;
         L.main_kind = 0;
@@ -565,7 +481,7 @@ scb_status for_each_chunk(scb_ctx* ctx, const uint8_t* seqs, const uint64_t* off
 // ---------------------------------------------------------------------------------------
 extern "C" {
 
-const char* scb_last_error(void) { return g_last_error.c_str(); }
+const char* scb_last_error(void) { return last_error_slot().c_str(); }
 const char* scb_version(void) { return "scb_b200 0.1.0 (sm_100a)"; }
 uint64_t scb_kernel_launches(void) { return kernel_launch_count(); }
 
@@ -800,6 +716,33 @@ scb_status scb_query_batch_device(scb_ctx* ctx, const uint8_t* d_seqs, const uin
     return read_counters(ctx, L, st, c);
 }
 
+// Build from one staged batch, freeze, then stream-query the same staged batch.
+static scb_status build_stream_batch(scb_ctx* ctx, Lane& L, const uint8_t* d_seqs, const uint64_t* d_offsets,
+                                     uint64_t n, uint64_t n_bytes, cudaStream_t st, uint64_t* kmers,
+                                     uint64_t* smers, scb_report* rep) {
+    TileArgs a;
+    SCB_TRY(prepare_batch(ctx, L, d_seqs, d_offsets, n, n_bytes, st, a));
+    SCB_TRY(insert_device_batch(ctx, L, a, st));
+    unsigned long long c1[kCntSlots];
+    SCB_TRY(read_counters(ctx, L, st, c1));
+    ctx->inserted_kmers += c1[kCntWindows];
+    ctx->inserted_smers += c1[kCntSmers];
+    ctx->frozen = true;
+    SCB_CUDA(cudaMemsetAsync(L.cnt.p, 0, kCntSlots * 8, st));
+    launch_seq_windows(a.offsets, n, ctx->g.k, a.cnt, nullptr, st);
+    SCB_TRY(query_device_batch(ctx, L, kModeReport, a, st));
+    unsigned long long c2[kCntSlots];
+    SCB_TRY(read_counters(ctx, L, st, c2));
+    if (kmers) *kmers = c1[kCntWindows];
+    if (smers) *smers = c1[kCntSmers];
+    rep->records_processed = c2[kCntRecords];
+    rep->total_windows = c2[kCntTotalWindows];
+    rep->valid_kmers = c2[kCntValid];
+    rep->positive_estimates = c2[kCntPositive];
+    rep->estimate_checksum = c2[kCntChecksum];
+    return SCB_OK;
+}
+
 scb_status scb_build_and_stream_query(scb_ctx* ctx, const uint8_t* seqs, const uint64_t* offsets, uint64_t n,
                                       uint64_t* kmers, uint64_t* smers, scb_report* rep) {
     if (!ctx || !rep) return fail_kind(SCB_ERR_INTERNAL_STATE, "null argument");
@@ -809,36 +752,31 @@ scb_status scb_build_and_stream_query(scb_ctx* ctx, const uint8_t* seqs, const u
         SCB_TRY(check_offsets(offsets, n));
         const uint64_t total = n ? offsets[n] - offsets[0] : 0;
         if (total <= kMaxBatchBytes - 64) {
-            // one resident batch: copy once, insert, freeze, query the same staged codes
+            // one resident batch: copy once, insert, freeze, query the same staged codes (and,
+            // with the grouped strategy, the same super-k-mer records)
             Lane& L = ctx->lane;
             Chunk c{0, n, n ? offsets[0] : 0, n ? offsets[n] : 0, 0};
             SCB_TRY(upload_chunk(ctx, L, seqs, offsets, c));
-            TileArgs a;
-            SCB_TRY(prepare_batch(ctx, L, L.ascii.as<uint8_t>(), L.offsets.as<uint64_t>(), n, total, L.stream, a));
-            SCB_TRY(insert_device_batch(ctx, L, a, L.stream));
-            unsigned long long c1[kCntSlots];
-            SCB_TRY(read_counters(ctx, L, L.stream, c1));
-            ctx->inserted_kmers += c1[kCntWindows];
-            ctx->inserted_smers += c1[kCntSmers];
-            ctx->frozen = true;
-            SCB_CUDA(cudaMemsetAsync(L.cnt.p, 0, kCntSlots * 8, L.stream));
-            launch_seq_windows(a.offsets, n, ctx->g.k, a.cnt, nullptr, L.stream);
-            SCB_TRY(query_device_batch(ctx, L, kModeReport, a, L.stream));
-            unsigned long long c2[kCntSlots];
-            SCB_TRY(read_counters(ctx, L, L.stream, c2));
-            if (kmers) *kmers = c1[kCntWindows];
-            if (smers) *smers = c1[kCntSmers];
-            rep->records_processed = c2[kCntRecords];
-            rep->total_windows = c2[kCntTotalWindows];
-            rep->valid_kmers = c2[kCntValid];
-            rep->positive_estimates = c2[kCntPositive];
-            rep->estimate_checksum = c2[kCntChecksum];
-            return SCB_OK;
+            return build_stream_batch(ctx, L, L.ascii.as<uint8_t>(), L.offsets.as<uint64_t>(), n, total, L.stream,
+                                      kmers, smers, rep);
         }
     }
     SCB_TRY(scb_insert_batch(ctx, seqs, offsets, n, kmers, smers));
     SCB_TRY(scb_freeze(ctx));
     return scb_query_report(ctx, seqs, offsets, n, rep);
+}
+
+scb_status scb_build_and_stream_query_device(scb_ctx* ctx, const uint8_t* d_seqs, const uint64_t* d_offsets,
+                                             uint64_t n, uint64_t n_bytes, void* stream, uint64_t* kmers,
+                                             uint64_t* smers, scb_report* rep) {
+    if (!ctx || !rep) return fail_kind(SCB_ERR_INTERNAL_STATE, "null argument");
+    CtxLock lk(ctx);
+    if (ctx->frozen) return fail_kind(SCB_ERR_INTERNAL_STATE, "the index is frozen; inserts need a builder");
+    if (n_bytes > kMaxBatchBytes - 64) return fail_kind(SCB_ERR_INTERNAL_STATE, "device batch above 2 GiB");
+    Lane& L = ctx->lane;
+    SCB_TRY(ensure_lane(ctx, L, n_bytes, n));
+    return build_stream_batch(ctx, L, d_seqs, d_offsets, n, n_bytes, reinterpret_cast<cudaStream_t>(stream), kmers,
+                              smers, rep);
 }
 
 // Rows of a dense histogram plus an overflow list, sorted by value, zero counts dropped.
@@ -1004,7 +942,9 @@ scb_status scb_set_timing(scb_ctx* ctx, int enable) {
     ctx->timing = enable != 0;
     ctx->times = scb_timings{};
     ctx->lane.pack_timed = false;
+    ctx->lane.cut_timed = false;
     ctx->lane.main_kind = 0;
+    ctx->lane.grouped_kind = 0;
     return SCB_OK;
 }
 

@@ -20,6 +20,7 @@
 // computes per super-k-mer.
 #include <atomic>
 #include <cstdio>
+#include <type_traits>
 
 #include "scb_kernels.cuh"
 
@@ -172,18 +173,78 @@ constexpr int kCodeWordsMax = (kEvalMax + 96 + 16) / 16 + 8;
 constexpr int kBitWordsMax = (kEvalMax + 128 + 32) / 32 + 8;
 constexpr uint16_t kNoWindow = 0xFFFFu;
 
+constexpr int kNtChunks = 11;  // ceil(32 / 3) 3-base chunks of an m-mer
+
 struct TileSmem {
     uint32_t codes[kCodeWordsMax];
     uint32_t valid[kBitWordsMax];
     uint32_t start[kBitWordsMax];
-    uint16_t key[kKeysMax];
+    uint32_t pk[kKeysMax];  // packed m-mer key: (hash >> 16) << 16 | position relative to e0
     uint16_t poff[kEvalMax];
     uint32_t block[kEvalMax];
     uint16_t ends[kTileWindows];
+    // canonical ntHash tables: 3-base chunk contributions (fw, rc) and one-base roll terms
+    uint32_t nt3f[kNtChunks * 64];
+    uint32_t nt3r[kNtChunks * 64];
+    uint32_t rollf[16];
+    uint32_t rollr[16];
     uint32_t n_ends;
     uint32_t tile;
     uint64_t seq_lo, seq_hi;
+    // cut mode: record slots reserved by this CTA in chunks (one global atomic per chunk)
+    uint64_t chunk_base, tile_base;
+    uint32_t chunk_used, chunk_cap;
+    uint32_t warp_cnt[kTileThreads / 32];
 };
+
+constexpr uint32_t kRecChunk = 4096;                // record slots reserved per global atomic
+constexpr unsigned long long kRecInvalid = ~0ull;  // unused reserved slot
+
+// Fills the per-CTA ntHash tables for m-mers of length m:
+//   nt3f[c][x] = XOR over bases t of chunk c of rotl(seed(base), 7 * (m - 1 - (3c + t)))
+//   nt3r[c][x] = XOR over bases t of chunk c of rotl(seed(base ^ 2), 7 * (3c + t))
+//   rollf[o | i << 2] = rotl(seed(o), 7m) ^ seed(i)
+//   rollr[o | i << 2] = rotr(seed(o ^ 2), 7) ^ rotl(seed(i ^ 2), 7(m - 1))
+// so that fw / rc of an m-mer are XORs of ceil(m/3) lookups and one base rolls in two.
+__device__ void fill_nt_tables(TileSmem& sm, uint32_t m) {
+    for (uint32_t e = threadIdx.x; e < kNtChunks * 64; e += blockDim.x) {
+        const uint32_t c = e >> 6, x = e & 63;
+        uint32_t f = 0, r = 0;
+        for (uint32_t t = 0; t < 3; t++) {
+            const uint32_t u = 3 * c + t;
+            if (u >= m) break;
+            const uint32_t b = (x >> (2 * t)) & 3u;
+            f ^= rotl32(nt_seed(b), kNtRot * (m - 1 - u));
+            r ^= rotl32(nt_seed(b ^ 2u), kNtRot * u);
+        }
+        sm.nt3f[e] = f;
+        sm.nt3r[e] = r;
+    }
+    if (threadIdx.x < 16) {
+        const uint32_t o = threadIdx.x & 3u, i = threadIdx.x >> 2;
+        sm.rollf[threadIdx.x] = rotl32(nt_seed(o), kNtRot * m) ^ nt_seed(i);
+        sm.rollr[threadIdx.x] = rotr32(nt_seed(o ^ 2u), kNtRot) ^ rotl32(nt_seed(i ^ 2u), kNtRot * (m - 1));
+    }
+}
+
+// Canonical ntHash key of the m-mer whose 2-bit codes are in v (masked to m bases).
+__device__ __forceinline__ void nt_direct_tab(const TileSmem& sm, uint64_t v, uint32_t m, uint32_t& fw,
+                                              uint32_t& rc) {
+    fw = 0;
+    rc = 0;
+    const uint32_t nch = (m + 2) / 3;
+    for (uint32_t c = 0; c < nch; c++) {
+        const uint32_t x = (uint32_t)(v >> (6 * c)) & 63u;
+        fw ^= sm.nt3f[c * 64 + x];
+        rc ^= sm.nt3r[c * 64 + x];
+    }
+}
+
+// Block id of the super-k-mer whose minimizer m-mer starts at relative base b.
+__device__ __forceinline__ uint32_t minimizer_block(const uint32_t* codes_s, uint64_t b, const DevGeom& g) {
+    const uint64_t mm = codes64(codes_s, b) & len_mask(g.m);
+    return (uint32_t)(xorshift64(canonical(mm, g.m)) & g.block_mask);
+}
 
 __device__ __forceinline__ uint32_t code_at(const uint32_t* words, uint64_t b) {
     return (words[b >> 4] >> (2 * (b & 15))) & 3u;
@@ -240,6 +301,15 @@ __global__ void __launch_bounds__(kTileThreads) k_tiles(TileArgs a) {
     unsigned long long c_win = 0, c_smer = 0, c_valid = 0, c_pos = 0, c_sum = 0, c_sk = 0, c_sec = 0, c_dist = 0;
     const uint64_t s_mask = len_mask(g.s);
     const uint32_t ks = g.k - g.s;
+    // modes that read a block id for every valid window (the cut computes it at ends only)
+    constexpr bool kBlockPerWindow = MODE == kModeInsert || MODE == kModeReport || MODE == kModeAbund ||
+                                     MODE == kModeDistinct || MODE == kModeMaterialize;
+    fill_nt_tables(sm, g.m);
+    if (MODE == kModeCut && tid == 0) {
+        sm.chunk_base = 0;
+        sm.chunk_used = 0;
+        sm.chunk_cap = 0;
+    }
 
     while (true) {
         if (tid == 0) sm.tile = atomicAdd(a.tile_counter, 1u);
@@ -277,45 +347,47 @@ __global__ void __launch_bounds__(kTileThreads) k_tiles(TileArgs a) {
         if (tid == 0) sm.n_ends = 0;
         __syncthreads();
 
-        // canonical m-mer hash keys (upper 16 bits) for m-mer positions e0 .. e0 + n_keys - 1
+        // canonical m-mer hash keys for m-mer positions e0 .. e0 + n_keys - 1, packed as
+        // (hash >> 16) << 16 | position so that one integer min picks the leftmost minimum
         {
-            const uint32_t per = (n_keys + blockDim.x - 1) / blockDim.x;
+            const uint32_t per = (n_keys + blockDim.x - 1) / blockDim.x;  // <= 5 with 1024-window tiles
             const uint32_t q0 = tid * per;
             const uint32_t q1 = min(q0 + per, n_keys);
             if (q0 < q1) {
                 const uint64_t b0 = e0 + q0 - cb;
                 uint32_t fw, rc;
-                nt_direct(codes64(sm.codes, b0) & len_mask(g.m), g.m, fw, rc);
-                sm.key[q0] = (uint16_t)((fw + rc) >> 16);
+                uint64_t outs = codes64(sm.codes, b0);  // bases leaving: b0, b0+1, ...
+                nt_direct_tab(sm, outs & len_mask(g.m), g.m, fw, rc);
+                sm.pk[q0] = ((fw + rc) & 0xFFFF0000u) | q0;
+                uint64_t ins = codes64(sm.codes, b0 + g.m);  // bases entering: b0+m, b0+m+1, ...
                 for (uint32_t q = q0 + 1; q < q1; q++) {
-                    const uint64_t b = e0 + q - cb;
-                    nt_roll(fw, rc, code_at(sm.codes, b - 1), code_at(sm.codes, b + g.m - 1), g.m);
-                    sm.key[q] = (uint16_t)((fw + rc) >> 16);
+                    const uint32_t idx = ((uint32_t)outs & 3u) | (((uint32_t)ins & 3u) << 2);
+                    outs >>= 2;
+                    ins >>= 2;
+                    fw = rotl32(fw, kNtRot) ^ sm.rollf[idx];
+                    rc = rotr32(rc, kNtRot) ^ sm.rollr[idx];
+                    sm.pk[q] = ((fw + rc) & 0xFFFF0000u) | q;
                 }
             }
         }
         __syncthreads();
 
-        // (b) minimizer of each evaluated window and its block
+        // (b) minimizer of each evaluated window: leftmost minimum = min(pk), rightmost minimum =
+        // min(pk ^ 0xFFFF) (the position bits inverted); strand from the count of T/G bases
         for (uint32_t i = tid; i < n_eval; i += blockDim.x) {
             const uint64_t pos = e0 + i;
             uint16_t po = kNoWindow;
             if (window_ok(bits64(sm.valid, pos - bb), bits64(sm.start, pos - bb), g.k)) {
-                uint32_t best = 0xFFFFFFFFu, left = 0, right = 0;
+                uint32_t lmin = 0xFFFFFFFFu, rmin = 0xFFFFFFFFu;
                 for (uint32_t o = 0; o < g.w; o++) {
-                    const uint32_t key = sm.key[i + o];
-                    if (key < best) {
-                        best = key;
-                        left = right = o;
-                    } else if (key == best) {
-                        right = o;
-                    }
+                    const uint32_t p = sm.pk[i + o];
+                    lmin = min(lmin, p);
+                    rmin = min(rmin, p ^ 0xFFFFu);
                 }
                 const uint64_t kv = codes64(sm.codes, pos - cb) & len_mask(g.k);
                 const uint32_t tg = __popcll(kv & 0xAAAAAAAAAAAAAAAAull);
-                po = (uint16_t)(i + ((2 * tg > g.k) ? left : right));
-                const uint64_t mm = codes64(sm.codes, e0 + po - cb) & len_mask(g.m);
-                sm.block[i] = (uint32_t)(xorshift64(canonical(mm, g.m)) & g.block_mask);
+                po = (uint16_t)((2 * tg > g.k) ? (lmin & 0xFFFFu) : ((rmin & 0xFFFFu) ^ 0xFFFFu));
+                if constexpr (kBlockPerWindow) sm.block[i] = minimizer_block(sm.codes, e0 + po - cb, g);
             }
             sm.poff[i] = po;
         }
@@ -411,10 +483,56 @@ __global__ void __launch_bounds__(kTileThreads) k_tiles(TileArgs a) {
                 }
             }
         } else if constexpr (MODE == kModeCut) {
-            // one record per super-k-mer, emitted at its last window: (block, first window, windows)
-            const uint32_t lane = tid & 31;
-            for (uint32_t r = 0; r < kTileWindows / kTileThreads; r++) {
-                const uint32_t i = back + r * kTileThreads + tid;
+            // one record per super-k-mer, emitted at its last window: (block, first window, windows).
+            // Slots: thread-contiguous within the tile, the tile's run taken from this CTA's chunk.
+            constexpr uint32_t kPer = kTileWindows / kTileThreads;
+            const uint32_t lane = tid & 31, wid = tid >> 5;
+            uint32_t mine = 0;  // ends among this thread's windows back + tid*kPer .. + kPer - 1
+            for (uint32_t r = 0; r < kPer; r++) {
+                const uint32_t i = back + tid * kPer + r;
+                const uint16_t po = sm.poff[i];
+                mine += (po != kNoWindow && sm.poff[i + 1] != po) ? 1u : 0u;
+            }
+            uint32_t incl = mine;
+            for (int off = 1; off < 32; off <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, off);
+                if ((int)lane >= off) incl += y;
+            }
+            if (lane == 31) sm.warp_cnt[wid] = incl;
+            __syncthreads();
+            uint32_t before = incl - mine, tile_total = 0;
+            for (uint32_t x = 0; x < kTileThreads / 32; x++) {
+                const uint32_t c = sm.warp_cnt[x];
+                before += x < wid ? c : 0u;
+                tile_total += c;
+            }
+            if (tid == 0) {
+                if (sm.chunk_used + tile_total > sm.chunk_cap) {
+                    // retire the rest of the current chunk (marked below) and reserve a new one
+                    const uint32_t want = tile_total > kRecChunk ? tile_total : kRecChunk;
+                    sm.tile_base = sm.chunk_base + sm.chunk_used;  // start of the retired rest
+                    sm.n_ends = sm.chunk_cap - sm.chunk_used;      // its length
+                    sm.chunk_base = atomicAdd(a.rec_count, (unsigned long long)want);
+                    sm.chunk_cap = want;
+                    sm.chunk_used = 0;
+                } else {
+                    sm.n_ends = 0;
+                }
+            }
+            __syncthreads();
+            for (uint32_t x = tid; x < sm.n_ends; x += blockDim.x) {
+                const unsigned long long slot = sm.tile_base + x;
+                if (slot < a.rec_cap) a.rec_val[slot] = kRecInvalid;
+            }
+            __syncthreads();
+            if (tid == 0) {
+                sm.tile_base = sm.chunk_base + sm.chunk_used;
+                sm.chunk_used += tile_total;
+            }
+            __syncthreads();
+            unsigned long long slot = sm.tile_base + before;
+            for (uint32_t r = 0; r < kPer; r++) {
+                const uint32_t i = back + tid * kPer + r;
                 const uint16_t po = sm.poff[i];
                 const bool valid = po != kNoWindow;
                 const bool end = valid && sm.poff[i + 1] != po;
@@ -427,21 +545,12 @@ __global__ void __launch_bounds__(kTileThreads) k_tiles(TileArgs a) {
                 if (end) {
                     c_sk++;
                     c_smer += nwin + ks;
-                }
-                const unsigned mask = __ballot_sync(0xFFFFFFFFu, end);
-                unsigned long long base = 0;
-                if (mask) {
-                    const int leader = __ffs(mask) - 1;
-                    if ((int)lane == leader) base = atomicAdd(a.rec_count, (unsigned long long)__popc(mask));
-                    base = __shfl_sync(0xFFFFFFFFu, base, leader);
-                }
-                if (end) {
-                    const unsigned long long slot = base + __popc(mask & ((1u << lane) - 1u));
-                    const uint32_t block = sm.block[i];
+                    const uint32_t block = minimizer_block(sm.codes, e0 + po - cb, g);
                     if (slot < a.rec_cap) {
                         a.rec_key[slot] = block;
                         a.rec_val[slot] = (unsigned long long)(e0 + st) | ((unsigned long long)nwin << kRecWindowsShift);
                     }
+                    slot++;
                     atomicAdd(a.bucket_hist + (block >> a.bucket_shift), 1ull);
                 }
             }
@@ -460,6 +569,14 @@ __global__ void __launch_bounds__(kTileThreads) k_tiles(TileArgs a) {
             }
         }
         __syncthreads();
+    }
+    if constexpr (MODE == kModeCut) {
+        // mark the unused rest of this CTA's last chunk (the loop ended after a barrier)
+        const uint64_t rest0 = sm.chunk_base + sm.chunk_used;
+        const uint32_t rest = sm.chunk_cap - sm.chunk_used;
+        for (uint32_t x = tid; x < rest; x += blockDim.x) {
+            if (rest0 + x < a.rec_cap) a.rec_val[rest0 + x] = kRecInvalid;
+        }
     }
     warp_add_u64(&a.cnt[kCntWindows], c_win);
     warp_add_u64(&a.cnt[kCntSmers], c_smer);
@@ -688,9 +805,11 @@ __global__ void k_scatter(const uint32_t* __restrict__ key, const unsigned long 
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     const uint32_t local_mask = (1u << shift) - 1u;
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const unsigned long long v = val[i];
+        if (v == kRecInvalid) continue;  // unused slot of a reserved chunk
         const uint32_t block = key[i];
         const unsigned long long pos = atomicAdd(cursor + (block >> shift), 1ull);
-        sorted[pos] = val[i] | ((unsigned long long)(block & local_mask) << kRecLocalShift);
+        sorted[pos] = v | ((unsigned long long)(block & local_mask) << kRecLocalShift);
     }
 }
 
@@ -779,19 +898,67 @@ __device__ __forceinline__ void chunk_prefix(const unsigned long long* rv, uint3
     __syncthreads();
 }
 
+template <int BITS>
+struct CounterType {
+    using type = uint32_t;
+};
+template <>
+struct CounterType<8> {
+    using type = uint8_t;
+};
+template <>
+struct CounterType<16> {
+    using type = uint16_t;
+};
+
+// Shared-memory layout of k_apply (offsets in bytes, all 16-byte aligned):
+//   cells   bucket counters: u32 deltas (insert) or the counters at native width (query)
+//   rv      the chunk's records
+//   spre    exclusive prefix of s-mers per record, wpre the same for windows
+//   smap    record of each s-mer of the chunk, wmap record of each window (query)
+//   touched one flag per block of the bucket
+//   est     s-mer minima of the chunk (query; 16-bit for 8/16-bit counters)
+struct ApplyLayout {
+    uint32_t cells, rv, spre, wpre, smap, wmap, touched, est, total;
+};
+
+__host__ __device__ inline uint32_t align16(uint32_t x) { return (x + 15u) & ~15u; }
+
+__host__ __device__ inline ApplyLayout apply_layout(int mode, int bits, uint32_t bucket_slots, uint32_t bucket_blocks) {
+    ApplyLayout l;
+    const uint32_t cell_bytes = mode == kModeInsert ? 4u : (uint32_t)bits / 8u;
+    const uint32_t max_smers = kApplyChunk * 62u, max_windows = kApplyChunk * 31u;
+    l.cells = 0;
+    l.rv = align16(bucket_slots * cell_bytes);
+    l.spre = l.rv + align16(kApplyChunk * 8u);
+    l.wpre = l.spre + align16((kApplyChunk + 1u) * 4u);
+    l.smap = l.wpre + align16((kApplyChunk + 1u) * 4u);
+    l.wmap = l.smap + align16(max_smers);
+    l.touched = l.wmap + (mode == kModeInsert ? 0u : align16(max_windows));
+    l.est = l.touched + align16(bucket_blocks);
+    l.total = l.est + (mode == kModeInsert ? 0u : align16(max_smers * (bits <= 16 ? 2u : 4u)));
+    return l;
+}
+
 template <int MODE, int BITS>
 __global__ void __launch_bounds__(kTileThreads) k_apply(GroupArgs a, uint32_t bs_log2, uint32_t bucket_blocks) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     using T = CounterTraits<BITS>;
+    using Cnt = typename CounterType<BITS>::type;
+    using Cell = typename std::conditional<MODE == kModeInsert, uint32_t, Cnt>::type;
+    using Est = typename std::conditional<(BITS <= 16), uint16_t, uint32_t>::type;
     const DevGeom g = a.g;
     const uint32_t bs = 1u << bs_log2;
     const uint32_t bucket_slots = bs * bucket_blocks;
-    uint32_t* cells = reinterpret_cast<uint32_t*>(smem_raw);
-    unsigned long long* rv = reinterpret_cast<unsigned long long*>(cells + ((bucket_slots + 3u) & ~3u));
-    uint32_t* spre = reinterpret_cast<uint32_t*>(rv + kApplyChunk);
-    uint32_t* wpre = spre + kApplyChunk + 4;
-    uint8_t* touched = reinterpret_cast<uint8_t*>(wpre + kApplyChunk + 4);
-    uint32_t* est = reinterpret_cast<uint32_t*>(touched + ((bucket_blocks + 15u) & ~15u));
+    const ApplyLayout lay = apply_layout(MODE, BITS, bucket_slots, bucket_blocks);
+    Cell* cells = reinterpret_cast<Cell*>(smem_raw + lay.cells);
+    unsigned long long* rv = reinterpret_cast<unsigned long long*>(smem_raw + lay.rv);
+    uint32_t* spre = reinterpret_cast<uint32_t*>(smem_raw + lay.spre);
+    uint32_t* wpre = reinterpret_cast<uint32_t*>(smem_raw + lay.wpre);
+    uint8_t* smap = smem_raw + lay.smap;
+    uint8_t* wmap = smem_raw + lay.wmap;
+    uint8_t* touched = smem_raw + lay.touched;
+    Est* est = reinterpret_cast<Est*>(smem_raw + lay.est);
     __shared__ uint4 item;
     __shared__ uint32_t warp_tot[2 * (kTileThreads / 32)];
 
@@ -828,7 +995,7 @@ __global__ void __launch_bounds__(kTileThreads) k_apply(GroupArgs a, uint32_t bs
                 const uint32_t lb = x >> bs_log2;
                 if (!touched[lb]) continue;
                 const uint64_t base = block_base(g, (bucket << a.bucket_shift) | lb);
-                cells[x] = load_counter<BITS>(a.table, base + (x & (bs - 1)));
+                cells[x] = (Cell)load_counter<BITS>(a.table, base + (x & (bs - 1)));
             }
             __syncthreads();
         }
@@ -838,15 +1005,24 @@ __global__ void __launch_bounds__(kTileThreads) k_apply(GroupArgs a, uint32_t bs
             if (tid < nrec) rv[tid] = a.recs[first + c0 + tid];
             __syncthreads();
             chunk_prefix(rv, nrec, ks, spre, wpre, warp_tot);
+            if (tid < nrec) {  // record index of every s-mer / window of the chunk
+                const uint32_t s0 = spre[tid], s1 = spre[tid + 1];
+                for (uint32_t f = s0; f < s1; f++) smap[f] = (uint8_t)tid;
+                if constexpr (MODE == kModeReport) {
+                    const uint32_t w0 = wpre[tid], w1 = wpre[tid + 1];
+                    for (uint32_t v = w0; v < w1; v++) wmap[v] = (uint8_t)tid;
+                }
+            }
+            __syncthreads();
             const uint32_t S = spre[nrec];
             for (uint32_t f = tid; f < S; f += blockDim.x) {
-                const uint32_t r = find_rec(spre, nrec, f);
+                const uint32_t r = smap[f];
                 const unsigned long long v = rv[r];
                 const uint64_t pos = (uint32_t)v + (f - spre[r]);
                 const uint32_t lb = (uint32_t)(v >> kRecLocalShift);
                 const uint64_t smer = canonical(codes64_ldg(a.codes, pos) & s_mask, g.s);
                 uint64_t hash = xorshift64(smer);
-                uint32_t* blk = cells + (lb << bs_log2);
+                Cell* blk = cells + (lb << bs_log2);
                 if constexpr (MODE == kModeInsert) {
                     for (uint32_t h = 0; h < g.h; h++) {
                         atomicAdd(blk + (hash & g.bs_mask), 1u);
@@ -860,18 +1036,17 @@ __global__ void __launch_bounds__(kTileThreads) k_apply(GroupArgs a, uint32_t bs
                         e = c < e ? c : e;
                         hash = xorshift64(hash);
                     }
-                    est[f] = e;
+                    est[f] = (Est)e;
                 }
             }
             __syncthreads();
             if constexpr (MODE == kModeReport) {
                 const uint32_t W = wpre[nrec];
                 for (uint32_t v = tid; v < W; v += blockDim.x) {
-                    const uint32_t r = find_rec(wpre, nrec, v);
-                    const uint32_t j = v - wpre[r];
-                    const uint32_t* e = est + spre[r] + j;
+                    const uint32_t r = wmap[v];
+                    const Est* e = est + spre[r] + (v - wpre[r]);
                     uint32_t m = e[0];
-                    for (uint32_t t = 1; t <= ks; t++) m = e[t] < m ? e[t] : m;
+                    for (uint32_t t = 1; t <= ks; t++) m = min(m, (uint32_t)e[t]);
                     c_valid++;
                     c_pos += m > 0;
                     c_sum += m;
@@ -918,17 +1093,14 @@ __global__ void __launch_bounds__(kTileThreads) k_apply(GroupArgs a, uint32_t bs
     warp_add_u64(&a.cnt[kCntChecksum], c_sum);
 }
 
-static size_t apply_smem(int mode, uint32_t bucket_slots, uint32_t bucket_blocks) {
-    size_t b = ((bucket_slots + 3u) & ~3u) * 4u + kApplyChunk * 8u + 2u * (kApplyChunk + 4u) * 4u +
-               ((bucket_blocks + 15u) & ~15u);
-    if (mode == kModeReport) b += (size_t)kApplyChunk * 64u * 4u;
-    return b;
+static size_t apply_smem(int mode, int bits, uint32_t bucket_slots, uint32_t bucket_blocks) {
+    return apply_layout(mode, bits, bucket_slots, bucket_blocks).total;
 }
 
 template <int MODE, int BITS>
 static void launch_apply_t(const GroupArgs& a, int bs_log2, uint32_t bucket_blocks, int sm_count, uint64_t max_items,
                            cudaStream_t st) {
-    const size_t smem = apply_smem(MODE, (1u << bs_log2) * bucket_blocks, bucket_blocks);
+    const size_t smem = apply_smem(MODE, BITS, (1u << bs_log2) * bucket_blocks, bucket_blocks);
     auto fn = k_apply<MODE, BITS>;
     cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int per_sm = 1;

@@ -272,14 +272,16 @@ def test_workload_medium_parity(scb, oracle_mod):
             oq.valid_kmers, oq.positive_estimates, oq.estimate_checksum)
 
 
-def test_build_and_stream_query_matches_separate_calls(scb, oracle_mod):
-    from scbf_b200 import _lib, workloads
+@pytest.mark.parametrize("strategy", ["auto", "plain", "fused", "grouped"])
+def test_build_and_stream_query_matches_separate_calls(scb, oracle_mod, strategy):
+    from scbf_b200 import _lib, api, workloads
     import ctypes as C
 
     data, offsets = workloads.short_reads(genome_len=100_000, n_reads=5_000, read_len=150, seed=3,
                                           sub_rate=0.01, n_rate=0.01)
     cfg = _cfg(scb, 31, 21, 25, 4, 22, 9, 16)
     b = scb.SuperCountingBloomBuilder(cfg)
+    api.set_strategy(b, strategy, strategy)
     km, sm = C.c_uint64(0), C.c_uint64(0)
     rep = _lib.ScbReport()
     st = _lib.load().scb_build_and_stream_query(b._ctx.h, data.ctypes.data, offsets.ctypes.data, len(offsets) - 1,
@@ -311,3 +313,36 @@ def test_errors_map_to_reference_variants(scb, tmp_path):
         b.set_threads(0)
     with pytest.raises(scb.FastxOpen):
         b.add_fasta(tmp_path / "missing.fa")
+
+
+@pytest.mark.parametrize("strategy", ["plain", "fused", "grouped"])
+def test_build_and_stream_query_device_matches_oracle(scb, oracle_mod, strategy):
+    import torch
+
+    from scbf_b200 import _lib, api, workloads
+    import ctypes as C
+
+    data, offsets = workloads.short_reads(genome_len=150_000, n_reads=8_000, read_len=150, seed=13,
+                                          sub_rate=0.01, n_rate=0.01)
+    o = oracle_mod.OracleFilter(oracle_mod.make_config(31, 21, 25, 4, 16, 22, 9))
+    okm, osm = o.insert_batch_arrays(data, offsets)
+    oq = o.query_report_arrays(data, offsets)
+    b = scb.SuperCountingBloomBuilder(_cfg(scb, 31, 21, 25, 4, 22, 9, 16))
+    api.set_strategy(b, strategy, strategy)
+    L = _lib.load()
+    d_data = torch.from_numpy(data).cuda()
+    d_off = torch.from_numpy(offsets.view(np.int64)).cuda()
+    km, sm = C.c_uint64(0), C.c_uint64(0)
+    rep = _lib.ScbReport()
+    for _ in range(2):  # a reset between steps gives the same result
+        assert L.scb_reset(b._ctx.h) == 0
+        st = L.scb_build_and_stream_query_device(b._ctx.h, d_data.data_ptr(), d_off.data_ptr(), len(offsets) - 1,
+                                                 int(offsets[-1]), None, C.byref(km), C.byref(sm), C.byref(rep))
+        assert st == 0, _lib.last_error()
+        assert (km.value, sm.value) == (okm, osm)
+        assert (rep.records_processed, rep.total_windows, rep.valid_kmers, rep.positive_estimates,
+                rep.estimate_checksum) == (oq.records_processed, oq.total_windows, oq.valid_kmers,
+                                           oq.positive_estimates, oq.estimate_checksum)
+        out = np.zeros(int(L.scb_table_bytes(b._ctx.h)), dtype=np.uint8)
+        assert L.scb_table_download(b._ctx.h, out.ctypes.data, out.size) == 0
+        assert np.array_equal(out.view(np.uint16), o.table())

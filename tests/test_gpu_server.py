@@ -1,0 +1,98 @@
+"""Serving loop: each request's abundances are identical alone, in a concurrent mix, and when
+the device-memory budget forces small batches and split requests -- and equal to the
+per-call query path."""
+import threading
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def index_and_requests():
+    import scbf_b200 as scb
+    from scbf_b200 import workloads
+
+    genome = workloads.random_genome(400_000, seed=31)
+    data, offsets = workloads.short_reads(n_reads=30_000, read_len=150, seed=32, sub_rate=0.01, n_rate=0.005,
+                                          genome=genome)
+    cfg = scb.SuperCountingBloomConfig(counter_slots_exponent=22, counter_bits=scb.CounterBits.Bits16)
+    b = scb.SuperCountingBloomBuilder(cfg)
+    b.add_sequences(data, offsets)
+    idx = b.into_index()
+    rng = np.random.default_rng(33)
+    requests = []
+    for i in range(40):
+        n = int(np.exp(rng.uniform(0, np.log(300))))
+        d, o = workloads.random_sequences(n, 20, 20_000, seed=100 + i, genome=genome)
+        if i % 7 == 3:  # runs of N inside some requests
+            d = d.copy()
+            d[rng.integers(0, d.size, max(1, d.size // 200))] = ord("N")
+        requests.append((d, o))
+    requests.append(scb.pack_sequences([b"", b"ACGT", b"N" * 50]))
+    expected = [idx.estimate_batch(d, o) for d, o in requests]
+    return idx, requests, expected
+
+
+def _check_all(results, expected):
+    for (out, valid), (eo, ev) in zip(results, expected):
+        assert np.array_equal(valid, ev)
+        assert np.array_equal(out, eo)
+
+
+def test_alone_equals_per_call_query(index_and_requests):
+    import scbf_b200 as scb
+
+    idx, requests, expected = index_and_requests
+    srv = scb.SuperCountingBloomServer(idx, max_batch_bytes=8 << 20, max_inflight=3)
+    results = []
+    for d, o in requests:
+        t = srv.submit(d, o)
+        out, valid, st = srv.wait(t)
+        assert st.total_ms >= st.service_ms >= 0
+        results.append((out, valid))
+    _check_all(results, expected)
+    summ = srv.summary()
+    assert summ["requests"] == len(requests) and summ["p99_ms"] >= summ["p50_ms"] > 0
+    srv.close()
+
+
+def test_concurrent_mix_equals_alone(index_and_requests):
+    import scbf_b200 as scb
+
+    idx, requests, expected = index_and_requests
+    srv = scb.SuperCountingBloomServer(idx, max_batch_bytes=4 << 20, max_inflight=4)
+    results = [None] * len(requests)
+    order = np.random.default_rng(5).permutation(len(requests))
+
+    def client(ids):
+        tickets = [(i, srv.submit(*requests[i])) for i in ids]  # submit all, then wait
+        for i, t in tickets:
+            out, valid, _ = srv.wait(t)
+            results[i] = (out, valid)
+
+    threads = [threading.Thread(target=client, args=(order[j::4].tolist(),)) for j in range(4)]
+    for th in threads:
+        th.start()
+    for th in threads:
+        th.join()
+    _check_all(results, expected)
+    assert srv.summary()["batches"] < len(requests)  # requests shared batches
+    srv.close()
+
+
+def test_memory_budget_admits_one_small_batch_at_a_time(index_and_requests):
+    import scbf_b200 as scb
+
+    idx, requests, expected = index_and_requests
+    # room for one slot of 256 KiB batches: big requests are split into many pieces
+    srv = scb.SuperCountingBloomServer(idx, memory_budget_bytes=4 << 20, max_batch_bytes=256 << 10,
+                                       max_inflight=8)
+    assert srv.summary()["slots"] == 1
+    tickets = [srv.submit(d, o) for d, o in requests]
+    results = [srv.wait(t)[:2] for t in tickets]
+    _check_all(results, expected)
+    srv.close()
+    with pytest.raises(scb.InvalidConfig, match="budget"):
+        scb.SuperCountingBloomServer(idx, memory_budget_bytes=1 << 20, max_batch_bytes=64 << 20)
