@@ -298,6 +298,13 @@ def run_ours(args, dist: Dist):
     check(L.scb_reset(h))
     check(L.scb_batch_stats(h, data.ctypes.data, offsets.ctypes.data, n_seqs, C.byref(st)))
 
+    # autotune on a sample of the workload (first 2 M reads) outside the timed region
+    tune = _lib.ScbTuning()
+    n_tune = min(n_seqs, 2_000_000)
+    t_tune = time.perf_counter()
+    check(L.scb_autotune(h, data.ctypes.data, offsets.ctypes.data, n_tune, C.byref(tune)))
+    tuning = dict(tune.as_dict(), sample_reads=n_tune, seconds=time.perf_counter() - t_tune)
+
     ms, info = timed("auto", args.steps)
     kmers = km.value
     assert rep.valid_kmers == kmers, (rep.valid_kmers, kmers)
@@ -409,6 +416,7 @@ def run_ours(args, dist: Dist):
             "query_kmers_per_s": kmers / (info["query_ms"] / 1e3),
             "stage_ms": {k_: info[k_] for k_ in ("pack_ms", "insert_ms", "query_ms", "cut_ms", "bucket_ms",
                                                  "apply_insert_ms", "apply_query_ms")},
+            "tuning": tuning,
             "plain": plain, "strategies": strategies, "mixed": mixed, "serve": serving, "e2e": e2e,
             "roofline": roofline,
             "cpu_baseline": cpu,

@@ -255,6 +255,30 @@ scb_status scb_server_reset_stats(scb_server* s);
 /* Drains in-flight batches, then frees the server (not the index). */
 void scb_server_destroy(scb_server* s);
 
+/* ---------------------------------------------------------------------------------------
+ * Autotuner (no counterpart in the reference).  Measures, on a sample of the caller's reads and
+ * a scratch table of the same geometry (the context's own table is not touched), the insert and
+ * query strategies for small and large batches (shared-memory staging of grouped blocks versus
+ * direct CAS atomics versus the plain pipeline), the grouped pipeline's records per bucket and
+ * apply CTA width (warps per work item), and the batch size of host calls (reads per batch).
+ * The result applies to the context's SCB_STRATEGY_AUTO and to every context created later in
+ * the process with the same (counter_bits, block_slots_exponent, counter_slots_exponent, k, m,
+ * s, n_hashes).  Results never change counters or estimates, only speed.
+ * --------------------------------------------------------------------------------------- */
+typedef struct scb_tuning {
+    uint64_t small_batch_bytes; /* batches below this use the *_small strategies */
+    int32_t insert_small, insert_large, query_small, query_large; /* scb_strategy values */
+    uint32_t bucket_records;  /* grouped: target super-k-mer records per bucket */
+    uint32_t apply_threads;   /* grouped: threads per apply CTA */
+    uint64_t host_batch_bytes; /* sequence bytes per device batch of a host call */
+    double insert_ms, query_ms; /* best times on the sample */
+    uint32_t candidates;       /* configurations measured */
+    uint32_t reserved;
+} scb_tuning;
+scb_status scb_autotune(scb_ctx* ctx, const uint8_t* seqs, const uint64_t* offsets, uint64_t n_seqs,
+                        scb_tuning* out);
+scb_status scb_get_tuning(const scb_ctx* ctx, scb_tuning* out);
+
 /* Clears the counter table and the insert totals and makes the context a builder again
  * (SuperCountingBloomBuilder::new on the existing allocation). */
 scb_status scb_reset(scb_ctx* ctx);

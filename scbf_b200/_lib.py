@@ -61,6 +61,22 @@ class ScbServerSummary(C.Structure):
                 ("span_s", C.c_double), ("slots", C.c_uint32), ("reserved", C.c_uint32)]
 
 
+class ScbTuning(C.Structure):
+    _fields_ = [("small_batch_bytes", C.c_uint64), ("insert_small", C.c_int32), ("insert_large", C.c_int32),
+                ("query_small", C.c_int32), ("query_large", C.c_int32), ("bucket_records", C.c_uint32),
+                ("apply_threads", C.c_uint32), ("host_batch_bytes", C.c_uint64), ("insert_ms", C.c_double),
+                ("query_ms", C.c_double), ("candidates", C.c_uint32), ("reserved", C.c_uint32)]
+
+    def as_dict(self) -> dict:
+        names = {v: k for k, v in STRATEGIES.items()}
+        return {"small_batch_bytes": self.small_batch_bytes, "insert_small": names.get(self.insert_small),
+                "insert_large": names.get(self.insert_large), "query_small": names.get(self.query_small),
+                "query_large": names.get(self.query_large), "bucket_records": self.bucket_records,
+                "apply_threads": self.apply_threads, "host_batch_bytes": self.host_batch_bytes,
+                "sample_insert_ms": self.insert_ms, "sample_query_ms": self.query_ms,
+                "candidates": self.candidates}
+
+
 _lib = None
 
 
@@ -127,6 +143,8 @@ def load(path: str | None = None):
         "scb_server_get_summary": (C.c_int, [vp, C.POINTER(ScbServerSummary)]),
         "scb_server_reset_stats": (C.c_int, [vp]),
         "scb_server_destroy": (None, [vp]),
+        "scb_autotune": (C.c_int, [ctxp, vp, vp, C.c_uint64, C.POINTER(ScbTuning)]),
+        "scb_get_tuning": (C.c_int, [ctxp, C.POINTER(ScbTuning)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -3,11 +3,16 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
+#include <cmath>
 #include <cstdio>
+#include <memory>
 #include <cstring>
 #include <mutex>
 #include <string>
 #include <thread>
+#include <map>
+#include <tuple>
 #include <vector>
 
 #include "../../include/scb.h"
@@ -181,22 +186,30 @@ bool grouped_supported(const scb_ctx* ctx) { return ctx->block_slots <= kMaxBuck
 // Expected super-k-mer records of a batch: about 2/(w+1) per window (random minimizers).
 uint64_t records_estimate(const scb_ctx* ctx, uint64_t n_bytes) { return n_bytes * 2 / (ctx->g.w + 1) + 1; }
 
-scb_strategy resolve(const scb_ctx* ctx, scb_strategy s, uint64_t n_bytes) {
+scb_strategy resolve(const scb_ctx* ctx, scb_strategy s, uint64_t n_bytes, bool insert) {
     if (s == SCB_STRATEGY_PLAIN || s == SCB_STRATEGY_FUSED) return s;
     if (s == SCB_STRATEGY_GROUPED) return grouped_supported(ctx) ? s : SCB_STRATEGY_FUSED;
-    // auto: grouping pays once a batch brings several super-k-mers per touched block
+    if (ctx->tuning.valid) {  // the autotuner's measured choice for this batch size
+        const bool small = n_bytes < ctx->tuning.small_bytes;
+        scb_strategy t = insert ? (small ? ctx->tuning.insert_small : ctx->tuning.insert_large)
+                                : (small ? ctx->tuning.query_small : ctx->tuning.query_large);
+        if (t == SCB_STRATEGY_GROUPED && !grouped_supported(ctx)) t = SCB_STRATEGY_FUSED;
+        return t;
+    }
+    // untuned: grouping pays once a batch brings about one super-k-mer per two blocks
     if (grouped_supported(ctx) && records_estimate(ctx, n_bytes) >= ctx->nb_blocks / 2) return SCB_STRATEGY_GROUPED;
     return SCB_STRATEGY_FUSED;
 }
 
 scb_strategy resolve(scb_strategy s) { return s == SCB_STRATEGY_AUTO ? SCB_STRATEGY_FUSED : s; }
 
-// Buckets of 2^shift consecutive blocks: about 512 records per bucket, at most 4096 counters
+// Buckets of 2^shift consecutive blocks: about tuning.bucket_records (512 untuned) records per
+// bucket, at most 4096 counters
 // (or one block when blocks are larger) staged in shared memory.
 uint32_t bucket_shift_for(const scb_ctx* ctx, uint64_t records) {
     uint32_t shift = 0;
     while ((ctx->block_slots << (shift + 1)) <= 4096 && (1ull << (shift + 1)) <= ctx->nb_blocks &&
-           records * (1ull << shift) / ctx->nb_blocks < 512) {
+           records * (1ull << shift) / ctx->nb_blocks < ctx->tuning.bucket_records) {
         shift++;
     }
     return shift;
@@ -292,6 +305,7 @@ scb_status grouped_prepare(scb_ctx* ctx, Lane& L, TileArgs& a, cudaStream_t st) 
     ga.n_items = reinterpret_cast<const unsigned long long*>(L.icount.as<uint64_t>() + n_buckets);
     ga.work_counter = L.tiles.as<unsigned int>() + 1;
     ga.bucket_shift = shift;
+    ga.apply_threads = ctx->tuning.apply_threads;
     if (ctx->timing) {
         SCB_CUDA(cudaEventRecord(L.ev[6], st));
         L.cut_timed = true;
@@ -325,7 +339,7 @@ scb_status run_grouped(scb_ctx* ctx, Lane& L, int mode, TileArgs& a, cudaStream_
 }
 
 scb_status insert_stage(scb_ctx* ctx, Lane& L, TileArgs& a, cudaStream_t st) {
-    const scb_strategy s = resolve(ctx, ctx->insert_strategy, a.n_bytes);
+    const scb_strategy s = resolve(ctx, ctx->insert_strategy, a.n_bytes, true);
     if (s == SCB_STRATEGY_GROUPED) return run_grouped(ctx, L, kModeInsert, a, st);
     if (s == SCB_STRATEGY_PLAIN) {
         SCB_TRY(run_materialize(ctx, L, a, st));
@@ -337,7 +351,7 @@ scb_status insert_stage(scb_ctx* ctx, Lane& L, TileArgs& a, cudaStream_t st) {
 }
 
 scb_status query_stage(scb_ctx* ctx, Lane& L, int mode, TileArgs& a, cudaStream_t st) {
-    const scb_strategy s = resolve(ctx, ctx->query_strategy, a.n_bytes);
+    const scb_strategy s = resolve(ctx, ctx->query_strategy, a.n_bytes, false);
     if (s == SCB_STRATEGY_GROUPED && mode == kModeReport) {
         // the lane's batch was already cut by a grouped insert of the same reads: reuse its records
         if (L.gs.valid) return grouped_apply(ctx, L, kModeReport, a.cnt, st);
@@ -423,6 +437,21 @@ struct CtxLock {
     explicit CtxLock(scb_ctx* c) : lk(c->mu) { cudaSetDevice(c->device); }
 };
 
+// Process-wide autotuner results, keyed by the geometry they were measured on.
+using TuneKey = std::tuple<uint8_t, uint8_t, uint8_t, uint64_t, uint64_t, uint64_t, uint64_t>;
+std::mutex g_tune_mu;
+std::map<TuneKey, Tuning> g_tune_cache;
+
+TuneKey tune_key(const scb_config& c) {
+    return TuneKey(c.counter_bits, c.block_slots_exponent, c.counter_slots_exponent, c.k, c.m, c.s, c.n_hashes);
+}
+
+void lookup_tuning(scb_ctx* ctx) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(tune_key(ctx->cfg));
+    if (it != g_tune_cache.end()) ctx->tuning = it->second;
+}
+
 scb_status alloc_ctx(const scb_config* cfg, scb_ctx** out) {
     SCB_TRY(validate_config(cfg));
     SCB_TRY(device_limits(cfg));
@@ -453,6 +482,7 @@ scb_status alloc_ctx(const scb_config* cfg, scb_ctx** out) {
         delete ctx;
         return fail_kind(SCB_ERR_INTERNAL_STATE, std::string("device setup failed: ") + cudaGetErrorString(e));
     }
+    lookup_tuning(ctx);
     *out = ctx;
     return SCB_OK;
 }
@@ -462,7 +492,7 @@ template <typename Fn>
 scb_status for_each_chunk(scb_ctx* ctx, const uint8_t* seqs, const uint64_t* offsets, uint64_t n, Fn&& fn) {
     SCB_TRY(check_offsets(offsets, n));
     std::vector<Chunk> chunks;
-    SCB_TRY(plan_chunks(offsets, n, ctx->cfg.k, kMaxBatchBytes - 64, chunks));
+    SCB_TRY(plan_chunks(offsets, n, ctx->cfg.k, ctx->tuning.host_batch_bytes, chunks));
     for (const Chunk& c : chunks) {
         Lane& L = ctx->lane;
         SCB_TRY(upload_chunk(ctx, L, seqs, offsets, c));
@@ -1138,6 +1168,166 @@ scb_status scb_load(const char* path, scb_ctx** out) {
     ctx->inserted_kmers = inserted;
     ctx->frozen = true;
     *out = ctx;
+    return SCB_OK;
+}
+
+
+static void tuning_to_public(const Tuning& t, scb_tuning* out) {
+    out->small_batch_bytes = t.small_bytes;
+    out->insert_small = t.insert_small;
+    out->insert_large = t.insert_large;
+    out->query_small = t.query_small;
+    out->query_large = t.query_large;
+    out->bucket_records = t.bucket_records;
+    out->apply_threads = t.apply_threads;
+    out->host_batch_bytes = t.host_batch_bytes;
+}
+
+scb_status scb_get_tuning(const scb_ctx* ctx, scb_tuning* out) {
+    if (!ctx || !out) return fail_kind(SCB_ERR_INTERNAL_STATE, "null argument");
+    std::memset(out, 0, sizeof(*out));
+    tuning_to_public(ctx->tuning, out);
+    return SCB_OK;
+}
+
+scb_status scb_autotune(scb_ctx* ctx, const uint8_t* seqs, const uint64_t* offsets, uint64_t n, scb_tuning* out) {
+    if (!ctx || !seqs || !offsets) return fail_kind(SCB_ERR_INTERNAL_STATE, "null argument");
+    SCB_TRY(check_offsets(offsets, n));
+    const uint64_t base = n ? offsets[0] : 0;
+    const uint64_t total = n ? offsets[n] - base : 0;
+    if (total == 0 || total > kMaxBatchBytes - 64)
+        return fail_kind(SCB_ERR_INTERNAL_STATE, "the autotuning sample must hold 1 byte to 2 GiB of sequences");
+    cudaSetDevice(ctx->device);
+    scb_ctx* scratch_raw = nullptr;
+    SCB_TRY(alloc_ctx(&ctx->cfg, &scratch_raw));
+    std::unique_ptr<scb_ctx> scratch(scratch_raw);
+    // the sample on the device, offsets rebased to its first byte
+    DevBuf d_seq, d_off;
+    SCB_TRY(d_seq.ensure(total + 64));
+    SCB_TRY(d_off.ensure((n + 1) * 8));
+    std::vector<uint64_t> off(offsets, offsets + n + 1);
+    for (auto& v : off) v -= base;
+    SCB_CUDA(cudaMemcpy(d_seq.p, seqs + base, total, cudaMemcpyHostToDevice));
+    SCB_CUDA(cudaMemcpy(d_off.p, off.data(), (n + 1) * 8, cudaMemcpyHostToDevice));
+    // small class: a prefix of about 1/32 of the sample (at least 64 KiB)
+    uint64_t n_small = 0;
+    const uint64_t small_target = std::max<uint64_t>(total / 32, 64 << 10);
+    while (n_small < n && off[n_small + 1] <= small_target) n_small++;
+    if (n_small == 0) n_small = 1;
+    const uint64_t small_bytes = off[n_small];
+
+    struct Cand {
+        scb_strategy s;
+        uint32_t bucket, threads;
+    };
+    uint32_t measured = 0;
+    // build + stream-query of the first nseq sequences with one candidate; second run timed
+    auto measure = [&](const Cand& c, uint64_t nseq, uint64_t nbytes, double& ins, double& q) -> scb_status {
+        scratch->insert_strategy = scratch->query_strategy = c.s;
+        scratch->tuning = Tuning();
+        scratch->tuning.bucket_records = c.bucket;
+        scratch->tuning.apply_threads = c.threads;
+        for (int rep = 0; rep < 2; rep++) {
+            SCB_TRY(scb_reset(scratch.get()));
+            SCB_TRY(scb_set_timing(scratch.get(), 1));
+            uint64_t km = 0, sm = 0;
+            scb_report r;
+            SCB_TRY(scb_build_and_stream_query_device(scratch.get(), d_seq.as<uint8_t>(), d_off.as<uint64_t>(), nseq,
+                                                      nbytes, nullptr, &km, &sm, &r));
+            scb_timings t;
+            SCB_TRY(scb_get_timings(scratch.get(), &t));
+            ins = t.pack_ms + t.insert_ms;
+            q = t.query_ms;
+        }
+        SCB_TRY(scb_set_timing(scratch.get(), 0));
+        measured++;
+        return SCB_OK;
+    };
+
+    std::vector<Cand> cands = {{SCB_STRATEGY_PLAIN, 512, 256}, {SCB_STRATEGY_FUSED, 512, 256}};
+    if (grouped_supported(ctx)) {
+        for (uint32_t b : {256u, 512u, 1024u, 2048u}) {
+            for (uint32_t t : {128u, 256u, 512u}) cands.push_back({SCB_STRATEGY_GROUPED, b, t});
+        }
+    }
+    Tuning best;
+    double best_ins = 1e30, best_q = 1e30, best_group = 1e30;
+    Cand best_ins_c = cands[1], best_q_c = cands[1], best_g_c = cands[1];
+    for (const Cand& c : cands) {
+        double ins = 0, q = 0;
+        SCB_TRY(measure(c, n, total, ins, q));
+        if (ins < best_ins) {
+            best_ins = ins;
+            best_ins_c = c;
+        }
+        if (q < best_q) {
+            best_q = q;
+            best_q_c = c;
+        }
+        if (c.s == SCB_STRATEGY_GROUPED && ins + q < best_group) {
+            best_group = ins + q;
+            best_g_c = c;
+        }
+    }
+    best.insert_large = best_ins_c.s;
+    best.query_large = best_q_c.s;
+    if (best_group < 1e30) {
+        best.bucket_records = best_g_c.bucket;
+        best.apply_threads = best_g_c.threads;
+    }
+    // small batches: the three strategies, grouped with the parameters chosen above
+    double s_ins = 1e30, s_q = 1e30;
+    for (scb_strategy st : {SCB_STRATEGY_PLAIN, SCB_STRATEGY_FUSED, SCB_STRATEGY_GROUPED}) {
+        if (st == SCB_STRATEGY_GROUPED && !grouped_supported(ctx)) continue;
+        double ins = 0, q = 0;
+        SCB_TRY(measure({st, best.bucket_records, best.apply_threads}, n_small, small_bytes, ins, q));
+        if (ins < s_ins) {
+            s_ins = ins;
+            best.insert_small = st;
+        }
+        if (q < s_q) {
+            s_q = q;
+            best.query_small = st;
+        }
+    }
+    const bool split = best.insert_small != best.insert_large || best.query_small != best.query_large;
+    // switch at the geometric midpoint of the two measured batch sizes
+    best.small_bytes = split ? (uint64_t)std::sqrt((double)small_bytes * (double)total) : 0;
+    // reads per batch of host calls: insert the whole sample through the host path in batches
+    // of a quarter, a half and all of it
+    best.valid = true;
+    double best_host = 1e30;
+    uint64_t best_chunk = best.host_batch_bytes;
+    for (uint64_t div : {4ull, 2ull, 1ull}) {
+        const uint64_t chunk = std::max<uint64_t>(total / div, 1 << 20);
+        scratch->tuning = best;
+        scratch->tuning.host_batch_bytes = chunk;
+        scratch->insert_strategy = scratch->query_strategy = SCB_STRATEGY_AUTO;
+        SCB_TRY(scb_reset(scratch.get()));
+        const auto t0 = std::chrono::steady_clock::now();
+        uint64_t km = 0, sm = 0;
+        SCB_TRY(scb_insert_batch(scratch.get(), seqs, offsets, n, &km, &sm));
+        const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        measured++;
+        if (ms < best_host) {
+            best_host = ms;
+            best_chunk = div == 1 ? kMaxBatchBytes - 64 : chunk;
+        }
+        if (chunk >= total) break;
+    }
+    best.host_batch_bytes = best_chunk;
+    ctx->tuning = best;
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune_cache[tune_key(ctx->cfg)] = best;
+    }
+    if (out) {
+        std::memset(out, 0, sizeof(*out));
+        tuning_to_public(best, out);
+        out->insert_ms = best_ins;
+        out->query_ms = best_q;
+        out->candidates = measured;
+    }
     return SCB_OK;
 }
 

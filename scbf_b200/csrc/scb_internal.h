@@ -119,6 +119,17 @@ struct Lane {
     }
 };
 
+// Choices of the autotuner (scb_autotune) for one geometry; defaults until tuned.
+struct Tuning {
+    bool valid = false;
+    uint64_t small_bytes = 0;  // batches below this many bytes use the *_small strategies
+    scb_strategy insert_small = SCB_STRATEGY_FUSED, insert_large = SCB_STRATEGY_GROUPED;
+    scb_strategy query_small = SCB_STRATEGY_FUSED, query_large = SCB_STRATEGY_GROUPED;
+    uint32_t bucket_records = 512;  // grouped: target super-k-mer records per bucket
+    uint32_t apply_threads = 256;   // grouped: CTA width of the apply kernel
+    uint64_t host_batch_bytes = kMaxBatchBytes - 64;  // sequence bytes per batch of a host call
+};
+
 }  // namespace scb
 
 struct scb_ctx {
@@ -136,6 +147,7 @@ struct scb_ctx {
     bool frozen = false;
     uint64_t inserted_kmers = 0, inserted_smers = 0;
     scb_strategy insert_strategy = SCB_STRATEGY_AUTO, query_strategy = SCB_STRATEGY_AUTO;
+    scb::Tuning tuning;
     scb::Lane lane;
     bool timing = false;
     scb_timings times{};

@@ -86,6 +86,78 @@ __global__ void k_pack(const uint8_t* __restrict__ ascii, uint64_t n, uint32_t* 
     }
 }
 
+// Graph-replayable packing: the batch's byte count comes from device memory (params[0]); the
+// launch covers the capacity of its shape class, groups past the batch write empty words.
+__global__ void k_pack_dyn(const uint8_t* __restrict__ ascii, const uint64_t* __restrict__ params,
+                           uint32_t* __restrict__ codes, uint32_t* __restrict__ valid, uint64_t cap_groups) {
+    const uint64_t n = params[0];
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t gi = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; gi < cap_groups; gi += stride) {
+        const uint64_t base = gi * 32;
+        uint32_t w[8];
+        if (base + 32 <= n) {
+            const uint4 x = __ldcs(reinterpret_cast<const uint4*>(ascii + base));
+            const uint4 y = __ldcs(reinterpret_cast<const uint4*>(ascii + base + 16));
+            w[0] = x.x; w[1] = x.y; w[2] = x.z; w[3] = x.w;
+            w[4] = y.x; w[5] = y.y; w[6] = y.z; w[7] = y.w;
+        } else {
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                uint32_t v = 0;
+                for (int b = 0; b < 4; b++) {
+                    const uint64_t idx = base + 4 * j + b;
+                    if (idx < n) v |= (uint32_t)ascii[idx] << (8 * b);
+                }
+                w[j] = v;
+            }
+        }
+        uint32_t c0 = 0, c1 = 0, vm = 0;
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            uint32_t c8, v4;
+            pack_word(w[j], c8, v4);
+            if (j < 4) {
+                c0 |= c8 << (8 * j);
+            } else {
+                c1 |= c8 << (8 * (j - 4));
+            }
+            vm |= v4 << (4 * j);
+        }
+        codes[2 * gi] = c0;
+        codes[2 * gi + 1] = c1;
+        valid[gi] = vm;
+    }
+}
+
+// Graph-replayable sequence starts: the sequence count comes from device memory (params[1]).
+__global__ void k_seqstart_dyn(const uint64_t* __restrict__ offsets, const uint64_t* __restrict__ params,
+                               uint32_t* __restrict__ seqstart) {
+    const uint64_t n_bytes = params[0], n_seqs = params[1];
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n_seqs; j += stride) {
+        const uint64_t a = offsets[j], b = offsets[j + 1];
+        if (b > a && a < n_bytes) atomicOr(&seqstart[a >> 5], 1u << (a & 31));
+    }
+}
+
+void launch_pack_dyn(const uint8_t* ascii, const uint64_t* params, uint64_t cap_bytes, uint32_t* codes,
+                     uint32_t* valid, cudaStream_t st) {
+    const uint64_t groups = (cap_bytes + 31) / 32;
+    if (groups == 0) return;
+    const uint64_t blocks = (groups + 255) / 256;
+    k_pack_dyn<<<(unsigned)(blocks < (1u << 20) ? blocks : (1u << 20)), 256, 0, st>>>(ascii, params, codes, valid,
+                                                                                      groups);
+    note_launch();
+}
+
+void launch_seqstart_dyn(const uint64_t* offsets, const uint64_t* params, uint64_t cap_seqs, uint32_t* seqstart,
+                         cudaStream_t st) {
+    if (cap_seqs == 0) return;
+    const uint64_t blocks = (cap_seqs + 255) / 256;
+    k_seqstart_dyn<<<(unsigned)(blocks < 65536 ? blocks : 65536), 256, 0, st>>>(offsets, params, seqstart);
+    note_launch();
+}
+
 __global__ void k_seqstart(const uint64_t* __restrict__ offsets, uint64_t n_seqs, uint64_t n_bytes,
                            uint32_t* __restrict__ seqstart) {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
@@ -250,6 +322,43 @@ __device__ __forceinline__ uint32_t code_at(const uint32_t* words, uint64_t b) {
     return (words[b >> 4] >> (2 * (b & 15))) & 3u;
 }
 
+// Window minimum of four consecutive windows i0..i0+3 (needs w >= 4): window i0+j covers the
+// packed keys [i0+j, i0+j+w-1] = suffix [i0+j, i0+3] of the first four keys, the middle
+// [i0+4, i0+w-1] shared by all four, and the first j keys of the tail [i0+w, i0+w+2].  Lout[j]
+// gets the minimum of the packed keys (leftmost minimum), Rout[j] of the keys with inverted
+// position bits (rightmost minimum).
+__device__ __forceinline__ void strip_minima(const uint32_t* pk, uint32_t i0, uint32_t w, uint32_t* Lout,
+                                             uint32_t* Rout) {
+    uint32_t a[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) a[j] = pk[i0 + j];
+    uint32_t sl[4], sr[4];
+    sl[3] = a[3];
+    sr[3] = a[3] ^ 0xFFFFu;
+#pragma unroll
+    for (int j = 2; j >= 0; j--) {
+        sl[j] = min(a[j], sl[j + 1]);
+        sr[j] = min(a[j] ^ 0xFFFFu, sr[j + 1]);
+    }
+    uint32_t ml = 0xFFFFFFFFu, mr = 0xFFFFFFFFu;
+    for (uint32_t o = 4; o < w; o++) {
+        const uint32_t p = pk[i0 + o];
+        ml = min(ml, p);
+        mr = min(mr, p ^ 0xFFFFu);
+    }
+    uint32_t pl = 0xFFFFFFFFu, pr = 0xFFFFFFFFu;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        if (j > 0) {
+            const uint32_t t = pk[i0 + w + j - 1];
+            pl = min(pl, t);
+            pr = min(pr, t ^ 0xFFFFu);
+        }
+        Lout[j] = min(min(sl[j], ml), pl);
+        Rout[j] = min(min(sr[j], mr), pr);
+    }
+}
+
 // Largest j in [lo, hi] with offsets[j] <= pos.
 __device__ __forceinline__ uint64_t seq_of(const uint64_t* offsets, uint64_t lo, uint64_t hi, uint64_t pos) {
     while (lo < hi) {
@@ -293,7 +402,7 @@ __device__ __forceinline__ uint32_t window_estimate(const TileArgs& a, const Dev
 }
 
 template <int MODE, int BITS>
-__global__ void __launch_bounds__(kTileThreads) k_tiles(TileArgs a) {
+__global__ void __launch_bounds__(kTileThreads, 8) k_tiles(TileArgs a) {
     __shared__ TileSmem sm;
     const DevGeom g = a.g;
     const uint32_t tid = threadIdx.x;
@@ -373,8 +482,31 @@ __global__ void __launch_bounds__(kTileThreads) k_tiles(TileArgs a) {
         __syncthreads();
 
         // (b) minimizer of each evaluated window: leftmost minimum = min(pk), rightmost minimum =
-        // min(pk ^ 0xFFFF) (the position bits inverted); strand from the count of T/G bases
-        for (uint32_t i = tid; i < n_eval; i += blockDim.x) {
+        // min(pk ^ 0xFFFF) (the position bits inverted); strand from the count of T/G bases.
+        // Windows 0..1023 go in strips of four per thread; the rest (and w < 4) one at a time.
+        const uint32_t strip_end = g.w >= 4 ? (uint32_t)kTileWindows : 0u;
+        if (strip_end) {
+            const uint32_t i0 = 4 * tid;
+            const uint64_t pos0 = e0 + i0;
+            const uint64_t vb = bits64(sm.valid, pos0 - bb), sb = bits64(sm.start, pos0 - bb);
+            uint32_t lm[4], rm[4];
+            strip_minima(sm.pk, i0, g.w, lm, rm);
+            uint32_t tg = __popcll(codes64(sm.codes, pos0 - cb) & len_mask(g.k) & 0xAAAAAAAAAAAAAAAAull);
+#pragma unroll
+            for (uint32_t j = 0; j < 4; j++) {
+                if (j > 0) {  // roll the T/G count by one base
+                    const uint64_t out_b = pos0 + j - 1 - cb;
+                    tg += (code_at(sm.codes, out_b + g.k) >> 1) - (code_at(sm.codes, out_b) >> 1);
+                }
+                uint16_t po = kNoWindow;
+                if (window_ok(vb >> j, sb >> j, g.k)) {
+                    po = (uint16_t)((2 * tg > g.k) ? (lm[j] & 0xFFFFu) : ((rm[j] & 0xFFFFu) ^ 0xFFFFu));
+                    if constexpr (kBlockPerWindow) sm.block[i0 + j] = minimizer_block(sm.codes, e0 + po - cb, g);
+                }
+                sm.poff[i0 + j] = po;
+            }
+        }
+        for (uint32_t i = strip_end + tid; i < n_eval; i += blockDim.x) {
             const uint64_t pos = e0 + i;
             uint16_t po = kNoWindow;
             if (window_ok(bits64(sm.valid, pos - bb), bits64(sm.start, pos - bb), g.k)) {
@@ -491,6 +623,7 @@ __global__ void __launch_bounds__(kTileThreads) k_tiles(TileArgs a) {
             for (uint32_t r = 0; r < kPer; r++) {
                 const uint32_t i = back + tid * kPer + r;
                 const uint16_t po = sm.poff[i];
+                c_win += po != kNoWindow;
                 mine += (po != kNoWindow && sm.poff[i + 1] != po) ? 1u : 0u;
             }
             uint32_t incl = mine;
@@ -505,6 +638,13 @@ __global__ void __launch_bounds__(kTileThreads) k_tiles(TileArgs a) {
                 const uint32_t c = sm.warp_cnt[x];
                 before += x < wid ? c : 0u;
                 tile_total += c;
+            }
+            // compact the tile's end windows, in window order, so the per-record work below runs
+            // on full warps
+            for (uint32_t r = 0; r < kPer; r++) {
+                const uint32_t i = back + tid * kPer + r;
+                const uint16_t po = sm.poff[i];
+                if (po != kNoWindow && sm.poff[i + 1] != po) sm.ends[before++] = (uint16_t)i;
             }
             if (tid == 0) {
                 if (sm.chunk_used + tile_total > sm.chunk_cap) {
@@ -530,29 +670,21 @@ __global__ void __launch_bounds__(kTileThreads) k_tiles(TileArgs a) {
                 sm.chunk_used += tile_total;
             }
             __syncthreads();
-            unsigned long long slot = sm.tile_base + before;
-            for (uint32_t r = 0; r < kPer; r++) {
-                const uint32_t i = back + tid * kPer + r;
+            for (uint32_t e = tid; e < tile_total; e += blockDim.x) {
+                const uint32_t i = sm.ends[e];
                 const uint16_t po = sm.poff[i];
-                const bool valid = po != kNoWindow;
-                const bool end = valid && sm.poff[i + 1] != po;
                 uint32_t st = i;
-                if (end) {
-                    while (st > 0 && sm.poff[st - 1] == po) st--;
-                }
+                while (st > 0 && sm.poff[st - 1] == po) st--;
                 const uint32_t nwin = i - st + 1;
-                c_win += valid;
-                if (end) {
-                    c_sk++;
-                    c_smer += nwin + ks;
-                    const uint32_t block = minimizer_block(sm.codes, e0 + po - cb, g);
-                    if (slot < a.rec_cap) {
-                        a.rec_key[slot] = block;
-                        a.rec_val[slot] = (unsigned long long)(e0 + st) | ((unsigned long long)nwin << kRecWindowsShift);
-                    }
-                    slot++;
-                    atomicAdd(a.bucket_hist + (block >> a.bucket_shift), 1ull);
+                c_sk++;
+                c_smer += nwin + ks;
+                const uint32_t block = minimizer_block(sm.codes, e0 + po - cb, g);
+                const unsigned long long slot = sm.tile_base + e;
+                if (slot < a.rec_cap) {
+                    a.rec_key[slot] = block;
+                    a.rec_val[slot] = (unsigned long long)(e0 + st) | ((unsigned long long)nwin << kRecWindowsShift);
                 }
+                atomicAdd(a.bucket_hist + (block >> a.bucket_shift), 1ull);
             }
         } else if constexpr (MODE == kModeDebugMin) {
             for (uint32_t i = tid; i < kTileWindows; i += blockDim.x) {
@@ -915,24 +1047,32 @@ struct CounterType<16> {
 //   cells   bucket counters: u32 deltas (insert) or the counters at native width (query)
 //   rv      the chunk's records
 //   spre    exclusive prefix of s-mers per record, wpre the same for windows
+//   bases   the 2-bit code words of each record of the chunk
 //   smap    record of each s-mer of the chunk, wmap record of each window (query)
 //   touched one flag per block of the bucket
 //   est     s-mer minima of the chunk (query; 16-bit for 8/16-bit counters)
 struct ApplyLayout {
-    uint32_t cells, rv, spre, wpre, smap, wmap, touched, est, total;
+    uint32_t cells, rv, spre, wpre, bases, smap, wmap, touched, est, total;
 };
+
+// s-mers (and windows) of one staged chunk of records; a record has at most 31 + 31
+constexpr uint32_t kSmerBudget = 2048;
+// 2-bit code words staged per record: its <= 62 bases from a 16-base boundary, plus the two
+// words codes64 reads past the last one
+constexpr uint32_t kRecBaseWords = 8;
 
 __host__ __device__ inline uint32_t align16(uint32_t x) { return (x + 15u) & ~15u; }
 
 __host__ __device__ inline ApplyLayout apply_layout(int mode, int bits, uint32_t bucket_slots, uint32_t bucket_blocks) {
     ApplyLayout l;
     const uint32_t cell_bytes = mode == kModeInsert ? 4u : (uint32_t)bits / 8u;
-    const uint32_t max_smers = kApplyChunk * 62u, max_windows = kApplyChunk * 31u;
+    const uint32_t max_smers = kSmerBudget, max_windows = kSmerBudget;
     l.cells = 0;
     l.rv = align16(bucket_slots * cell_bytes);
     l.spre = l.rv + align16(kApplyChunk * 8u);
     l.wpre = l.spre + align16((kApplyChunk + 1u) * 4u);
-    l.smap = l.wpre + align16((kApplyChunk + 1u) * 4u);
+    l.bases = l.wpre + align16((kApplyChunk + 1u) * 4u);
+    l.smap = l.bases + kApplyChunk * kRecBaseWords * 4u;
     l.wmap = l.smap + align16(max_smers);
     l.touched = l.wmap + (mode == kModeInsert ? 0u : align16(max_windows));
     l.est = l.touched + align16(bucket_blocks);
@@ -941,7 +1081,7 @@ __host__ __device__ inline ApplyLayout apply_layout(int mode, int bits, uint32_t
 }
 
 template <int MODE, int BITS>
-__global__ void __launch_bounds__(kTileThreads) k_apply(GroupArgs a, uint32_t bs_log2, uint32_t bucket_blocks) {
+__global__ void __launch_bounds__(kApplyMaxThreads) k_apply(GroupArgs a, uint32_t bs_log2, uint32_t bucket_blocks) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     using T = CounterTraits<BITS>;
     using Cnt = typename CounterType<BITS>::type;
@@ -955,12 +1095,13 @@ __global__ void __launch_bounds__(kTileThreads) k_apply(GroupArgs a, uint32_t bs
     unsigned long long* rv = reinterpret_cast<unsigned long long*>(smem_raw + lay.rv);
     uint32_t* spre = reinterpret_cast<uint32_t*>(smem_raw + lay.spre);
     uint32_t* wpre = reinterpret_cast<uint32_t*>(smem_raw + lay.wpre);
+    uint32_t* bases = reinterpret_cast<uint32_t*>(smem_raw + lay.bases);
     uint8_t* smap = smem_raw + lay.smap;
     uint8_t* wmap = smem_raw + lay.wmap;
     uint8_t* touched = smem_raw + lay.touched;
     Est* est = reinterpret_cast<Est*>(smem_raw + lay.est);
     __shared__ uint4 item;
-    __shared__ uint32_t warp_tot[2 * (kTileThreads / 32)];
+    __shared__ uint32_t warp_tot[2 * (kApplyMaxThreads / 32)];
 
     const uint32_t tid = threadIdx.x;
     const uint32_t ks = g.k - g.s;
@@ -1000,27 +1141,36 @@ __global__ void __launch_bounds__(kTileThreads) k_apply(GroupArgs a, uint32_t bs
             __syncthreads();
         }
 
-        for (uint32_t c0 = 0; c0 < count; c0 += kApplyChunk) {
+        for (uint32_t c0 = 0; c0 < count;) {
             const uint32_t nrec = min(kApplyChunk, count - c0);
             if (tid < nrec) rv[tid] = a.recs[first + c0 + tid];
             __syncthreads();
             chunk_prefix(rv, nrec, ks, spre, wpre, warp_tot);
-            if (tid < nrec) {  // record index of every s-mer / window of the chunk
+            // the leading records whose s-mers fit the chunk's budget (at least one)
+            const uint32_t nuse = (uint32_t)__syncthreads_count(tid < nrec && spre[tid + 1] <= kSmerBudget);
+            if (tid < nuse) {  // stage the record's bases; record index of its s-mers / windows
+                const unsigned long long v = rv[tid];
+                const uint64_t w0 = (uint32_t)v >> 4;
+                uint32_t* rb = bases + tid * kRecBaseWords;
+#pragma unroll
+                for (uint32_t x = 0; x < kRecBaseWords; x++) rb[x] = __ldg(a.codes + w0 + x);
                 const uint32_t s0 = spre[tid], s1 = spre[tid + 1];
                 for (uint32_t f = s0; f < s1; f++) smap[f] = (uint8_t)tid;
                 if constexpr (MODE == kModeReport) {
-                    const uint32_t w0 = wpre[tid], w1 = wpre[tid + 1];
-                    for (uint32_t v = w0; v < w1; v++) wmap[v] = (uint8_t)tid;
+                    const uint32_t w0i = wpre[tid], w1i = wpre[tid + 1];
+                    for (uint32_t vv = w0i; vv < w1i; vv++) wmap[vv] = (uint8_t)tid;
                 }
             }
             __syncthreads();
-            const uint32_t S = spre[nrec];
+            const uint32_t nrec_used = nuse;
+            const uint32_t S = spre[nrec_used];
             for (uint32_t f = tid; f < S; f += blockDim.x) {
                 const uint32_t r = smap[f];
                 const unsigned long long v = rv[r];
-                const uint64_t pos = (uint32_t)v + (f - spre[r]);
+                const uint32_t start = (uint32_t)v;
+                const uint32_t rel = (start & 15u) + (f - spre[r]);  // base offset in the staged words
                 const uint32_t lb = (uint32_t)(v >> kRecLocalShift);
-                const uint64_t smer = canonical(codes64_ldg(a.codes, pos) & s_mask, g.s);
+                const uint64_t smer = canonical(codes64(bases + r * kRecBaseWords, rel) & s_mask, g.s);
                 uint64_t hash = xorshift64(smer);
                 Cell* blk = cells + (lb << bs_log2);
                 if constexpr (MODE == kModeInsert) {
@@ -1041,7 +1191,7 @@ __global__ void __launch_bounds__(kTileThreads) k_apply(GroupArgs a, uint32_t bs
             }
             __syncthreads();
             if constexpr (MODE == kModeReport) {
-                const uint32_t W = wpre[nrec];
+                const uint32_t W = wpre[nrec_used];
                 for (uint32_t v = tid; v < W; v += blockDim.x) {
                     const uint32_t r = wmap[v];
                     const Est* e = est + spre[r] + (v - wpre[r]);
@@ -1053,6 +1203,7 @@ __global__ void __launch_bounds__(kTileThreads) k_apply(GroupArgs a, uint32_t bs
                 }
                 __syncthreads();
             }
+            c0 += nrec_used;
         }
 
         if constexpr (MODE == kModeInsert) {
@@ -1103,14 +1254,15 @@ static void launch_apply_t(const GroupArgs& a, int bs_log2, uint32_t bucket_bloc
     const size_t smem = apply_smem(MODE, BITS, (1u << bs_log2) * bucket_blocks, bucket_blocks);
     auto fn = k_apply<MODE, BITS>;
     cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const int threads = (a.apply_threads == 128 || a.apply_threads == 512) ? (int)a.apply_threads : 256;
     int per_sm = 1;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kTileThreads, smem) != cudaSuccess || per_sm < 1) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem) != cudaSuccess || per_sm < 1) {
         per_sm = 1;
     }
     uint64_t grid = (uint64_t)per_sm * sm_count;
     if (grid > max_items) grid = max_items;
     if (grid == 0) grid = 1;
-    fn<<<(unsigned)grid, kTileThreads, smem, st>>>(a, (uint32_t)bs_log2, bucket_blocks);
+    fn<<<(unsigned)grid, threads, smem, st>>>(a, (uint32_t)bs_log2, bucket_blocks);
     note_launch();
 }
 

@@ -33,6 +33,7 @@ constexpr uint32_t kRecLocalShift = 38;
 constexpr uint32_t kItemRecords = 4096;    // records per work item (heavier buckets are split)
 constexpr uint32_t kApplyChunk = 128;      // records staged in shared memory at a time
 constexpr uint32_t kMaxBucketSlots = 16384;  // counters of one bucket held in shared memory
+constexpr uint32_t kApplyMaxThreads = 512;
 
 struct GroupArgs {
     DevGeom g;
@@ -46,7 +47,7 @@ struct GroupArgs {
     const unsigned long long* n_items;
     unsigned int* work_counter;
     uint32_t bucket_shift;
-    uint32_t pad_;
+    uint32_t apply_threads;  // CTA width of the apply kernel: 128, 256 (default) or 512
 };
 
 // Slots of the per-launch 64-bit counter array.
@@ -109,6 +110,11 @@ struct TileArgs {
 
 // Kernel launches; each counts itself in the library-wide launch counter.
 void launch_pack(const uint8_t* ascii, uint64_t n_bytes, uint32_t* codes, uint32_t* valid, cudaStream_t st);
+// graph-replayable forms: sizes read from params[0] (bytes) / params[1] (sequences) on the device
+void launch_pack_dyn(const uint8_t* ascii, const uint64_t* params, uint64_t cap_bytes, uint32_t* codes,
+                     uint32_t* valid, cudaStream_t st);
+void launch_seqstart_dyn(const uint64_t* offsets, const uint64_t* params, uint64_t cap_seqs, uint32_t* seqstart,
+                         cudaStream_t st);
 void launch_seqstart(const uint64_t* offsets, uint64_t n_seqs, uint64_t n_bytes, uint32_t* seqstart,
                      cudaStream_t st);
 void launch_seq_windows(const uint64_t* offsets, uint64_t n_seqs, uint32_t k, unsigned long long* cnt,
