@@ -57,6 +57,8 @@ def parse():
     p.add_argument("--no-serve", action="store_true", help="skip the serving (config 5) measurement")
     p.add_argument("--profile-case", choices=["plain", "fused", "grouped"], default=None,
                    help="run one insert + query of a small case (for ncu) and exit")
+    p.add_argument("--profile-scale", type=float, default=0.1,
+                   help="genome scale of the profile case (1.0 = the full 2 Gbp workload)")
     return p.parse_args()
 
 
@@ -119,12 +121,18 @@ class Clocks:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
         except OSError:
             self.proc = None
+            return
+        # the timed region starts once the sampler is running (its first line is out)
+        t0 = time.perf_counter()
+        while not self.lines and self.proc.poll() is None and time.perf_counter() - t0 < 3.0:
+            time.sleep(0.01)
+        self.skip = len(self.lines)
 
     def _read(self):
         for line in self.proc.stdout:
@@ -140,7 +148,8 @@ class Clocks:
             self.proc.kill()
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        lines = self.lines[getattr(self, "skip", 0):] or self.lines[-1:]
+        for ln in lines:
             parts = [x.strip() for x in ln.split(",")]
             if len(parts) < 9:
                 continue
@@ -165,9 +174,10 @@ def measured_peaks() -> tuple[float, str]:
 
 
 def profile_traffic() -> dict | None:
-    """DRAM bytes per k-mer of the insert tile kernel from the committed ncu summary (a capture of
-    a smaller case, scaled per k-mer window to a full launch)."""
-    p = os.path.join(ROOT, "profiles", "insert_tile_traffic.json")
+    """Per-kernel DRAM bytes per launch of the grouped step on this workload, from the committed
+    one-pass ncu capture (profiles/traffic_grouped_config2.json), with the pipe that limits each
+    kernel from the full capture of the small case."""
+    p = os.path.join(ROOT, "profiles", "traffic_grouped_config2.json")
     try:
         return json.load(open(p))
     except (OSError, ValueError):
@@ -219,6 +229,12 @@ def run_reference(args, dist: Dist):
 
 # ---------------------------------------------------------------------------------------
 STRATEGY_IDS = {"auto": 0, "plain": 1, "fused": 2, "grouped": 4}
+
+
+def graph_stats(L, h) -> tuple[int, int, int]:
+    c, r, f = C.c_uint64(), C.c_uint64(), C.c_uint64()
+    assert L.scb_graph_stats(h, C.byref(c), C.byref(r), C.byref(f)) == 0
+    return c.value, r.value, f.value
 
 
 def occupied(n_items: float, n_bins: float) -> float:
@@ -276,10 +292,12 @@ def run_ours(args, dist: Dist):
         clocks = Clocks(dist.local)
         clocks.start()
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.nvtx.range_push("timed")  # lets a profiler capture the timed launches only
         ev0.record(stream)
         for _ in range(steps):
             step()
         ev1.record(stream)
+        torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize()
         clk = clocks.stop()
         dist.barrier()
@@ -305,7 +323,11 @@ def run_ours(args, dist: Dist):
     check(L.scb_autotune(h, data.ctypes.data, offsets.ctypes.data, n_tune, C.byref(tune)))
     tuning = dict(tune.as_dict(), sample_reads=n_tune, seconds=time.perf_counter() - t_tune)
 
+    g0 = graph_stats(L, h)
     ms, info = timed("auto", args.steps)
+    g1 = graph_stats(L, h)
+    graphs = {"captures": g1[0] - g0[0], "replays": g1[1] - g0[1], "eager_redos": g1[2] - g0[2],
+              "note": "every timed step is one graph replay of its batch shape (captured in warm-up)"}
     kmers = km.value
     assert rep.valid_kmers == kmers, (rep.valid_kmers, kmers)
     all_kmers = dist.sum(float(kmers))
@@ -343,37 +365,60 @@ def run_ours(args, dist: Dist):
         e2e = {"value": all_kmers * len(times) / sum(times), "unit": "k-mers/s",
                "h2d_bytes_per_step": n_bytes + (n_seqs + 1) * 8, "d2h_bytes_per_step": 2 * (16 * 8 + 4) + 8}
 
-    # roofline of the dominant kernel of the timed step
+    # roofline of the dominant kernel of the timed step.  Algorithmic bytes follow the
+    # random-32-byte-sector model of the direct design: each distinct sector that a super-k-mer's
+    # probes hit is read (and, for an insert, written) once per super-k-mer, plus the 2-bit
+    # packed reads; the report query writes no per-window output.  The grouped kernels stage each
+    # touched block once per bucket instead, so they can run above this roofline.
     peak, peak_kind = measured_peaks()
     R = float(st.super_kmers)
-    bytes_per = GEOM["counter_bits"] // 8
-    block_bytes = (1 << GEOM["block_slots_exponent"]) * bytes_per
-    nb_blocks = 1 << (GEOM["counter_slots_exponent"] - GEOM["block_slots_exponent"])
-    touched = occupied(R, nb_blocks)
-    gather = (st.windows + R * (GEOM["k"] - 1)) / 4.0  # 2-bit bases of every record
+    sector_bytes = 32.0 * st.sectors
+    packed = n_bytes / 4.0
+    alg_insert = 2.0 * sector_bytes + packed
+    alg_query = sector_bytes + packed
+    grouped_step = info["cut_ms"] > 0
     kernels = {
-        # one read of the packed codes and bitmaps, 12-byte record and 8-byte bucket count per super-k-mer
+        "k_apply<insert>": (info["apply_insert_ms"], alg_insert),
+        "k_apply<query>": (info["apply_query_ms"], alg_query),
+        # own bytes of the cut: codes and bitmaps read once, 12-byte record + 8-byte count each
         "k_tiles<cut>": (info["cut_ms"], n_bytes / 2 + 20 * R),
-        # sorted records + gathered bases + each touched block read and written once
-        "k_apply<insert>": (info["apply_insert_ms"], 8 * R + gather + 2 * touched * block_bytes),
-        # sorted records + gathered bases + each touched block read once
-        "k_apply<query>": (info["apply_query_ms"], 8 * R + gather + touched * block_bytes),
-        # random-sector bound of the direct design: each distinct 32-byte sector read + written
-        "k_tiles<insert>": (info["insert_ms"] if info["cut_ms"] == 0 else 0.0, 64 * st.sectors + n_bytes / 4),
+        # the fused strategy's tile kernels carry the whole stage
+        "k_tiles<insert>": (0.0 if grouped_step else info["insert_ms"], alg_insert),
+        "k_tiles<report>": (0.0 if grouped_step else info["query_ms"], alg_query),
     }
     dom = max(kernels, key=lambda k_: kernels[k_][0])
     dom_ms, alg = kernels[dom]
     achieved = alg / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
-    traffic = profile_traffic()
+    prof = profile_traffic() or {}
+    kprof = prof.get("kernels", {}).get(dom, {})
+    # bytes the grouped design needs at least: sorted records, the gathered bases of each record
+    # (read once), each touched block read (and written, insert) once
+    touched = occupied(R, float(1 << (GEOM["counter_slots_exponent"] - GEOM["block_slots_exponent"])))
+    block_bytes = (1 << GEOM["block_slots_exponent"]) * (GEOM["counter_bits"] // 8)
+    gather = (st.windows + R * (GEOM["k"] - 1)) / 4.0
+    staged_min = {"k_apply<insert>": 8 * R + gather + 2 * touched * block_bytes,
+                  "k_apply<query>": 8 * R + gather + touched * block_bytes}.get(dom)
+
+    def stage(ms, alg_b):
+        gbs = alg_b / (ms / 1e3) / 1e9 if ms > 0 else 0.0
+        return {"ms": ms, "achieved": gbs, "frac": gbs / peak,
+                "kmers_per_s": kmers / (ms / 1e3) if ms > 0 else 0.0,
+                "roofline_kmers_per_s": kmers / (alg_b / (peak * 1e9))}
+
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_kind": peak_kind,
-                "traffic": (traffic.get(dom, {}).get("dram_bytes_per_kmer", 0) * kmers) if traffic and dom in traffic
-                else None,
+                "traffic": kprof.get("dram_bytes_per_launch"),
+                "traffic_source": prof.get("source") if kprof else None,
                 "algorithmic_bytes": alg, "kernel_ms": dom_ms,
+                "algorithmic_model": "random 32-byte sectors: 32 B x distinct sectors per super-k-mer "
+                                     "(x2 for insert) + 2-bit packed reads",
+                "limiter": kprof.get("limiter"),
+                "staged_minimum_bytes": staged_min,
+                "staged_minimum_frac": (staged_min / (dom_ms / 1e3) / 1e9 / peak) if staged_min and dom_ms > 0
+                else None,
+                "stages": {"insert": stage(info["insert_ms"], alg_insert),
+                           "query": stage(info["query_ms"], alg_query)},
                 "kernels_ms": {k_: v[0] for k_, v in kernels.items()},
-                "random_sector_bound_kmers_per_s": {
-                    "insert": kmers / ((64 * st.sectors + n_bytes / 4) / (peak * 1e9)),
-                    "query": kmers / ((32 * st.sectors + n_bytes / 4 + 8 * kmers) / (peak * 1e9))},
                 "sectors_per_superkmer": st.sectors / max(st.super_kmers, 1),
                 "super_kmers": st.super_kmers, "smers": st.smers, "touched_blocks": touched}
 
@@ -416,7 +461,7 @@ def run_ours(args, dist: Dist):
             "query_kmers_per_s": kmers / (info["query_ms"] / 1e3),
             "stage_ms": {k_: info[k_] for k_ in ("pack_ms", "insert_ms", "query_ms", "cut_ms", "bucket_ms",
                                                  "apply_insert_ms", "apply_query_ms")},
-            "tuning": tuning,
+            "tuning": tuning, "graphs": graphs,
             "plain": plain, "strategies": strategies, "mixed": mixed, "serve": serving, "e2e": e2e,
             "roofline": roofline,
             "cpu_baseline": cpu,
@@ -519,9 +564,15 @@ def run_serving(ctx, args, rank: int) -> dict:
                 "batches": s.batches, "slots": s.slots,
                 "mean_kmers_per_request": float(np.mean([outs[j][2] for j in pick]))}
 
-    fixed = stream(pool_fixed(16), rate=300.0, seconds=3.0, max_batch_bytes=16 << 20)
+    fixed_pool = pool_fixed(16)
+    fixed = stream(fixed_pool, rate=300.0, seconds=3.0, max_batch_bytes=16 << 20)
     mixed = stream(pool_mixed(48), rate=100.0, seconds=3.0, max_batch_bytes=32 << 20)
-    return {"index": "config-2 frozen index, resident", "one_mkmer_requests": fixed, "mixed_requests": mixed}
+    # the same 1 M-k-mer stream with every batch launched kernel by kernel (no graph replays)
+    L.scb_set_graphs(ctx.h, 0)
+    fixed_eager = stream(fixed_pool, rate=300.0, seconds=3.0, max_batch_bytes=16 << 20)
+    L.scb_set_graphs(ctx.h, 1)
+    return {"index": "config-2 frozen index, resident", "one_mkmer_requests": fixed, "mixed_requests": mixed,
+            "one_mkmer_requests_without_graphs": fixed_eager}
 
 
 MIXED_WORKLOAD = ("mixed lengths: 200 Mbp uniform genome at 15x; 70% of bases from 150 bp reads (1% "
@@ -599,6 +650,23 @@ def run_mixed(args, dist: Dist) -> dict:
             ref = res
         assert res == ref, (name, res, ref)
         out[name] = dist.sum(float(res[0])) * steps / (ms / 1e3)
+    # the same tuned strategies with every batch launched eagerly (no graph replays)
+    check(L.scb_set_strategy(h, 0, 0))
+    check(L.scb_set_graphs(h, 0))
+    for _ in range(min(args.warmup, 2)):
+        step()
+    torch.cuda.synchronize()
+    dist.barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(max(1, args.steps // 2)):
+        res = step()
+    ev1.record()
+    torch.cuda.synchronize()
+    ms = dist.max(ev0.elapsed_time(ev1))
+    assert res == ref, ("auto without graphs", res, ref)
+    out["auto_without_graphs"] = dist.sum(float(res[0])) * max(1, args.steps // 2) / (ms / 1e3)
+    check(L.scb_set_graphs(h, 1))
     out["kmers_per_step"] = ref[0]
     out["batched_over_plain"] = out["auto"] / out["plain"]
     ctx.close()
@@ -606,14 +674,15 @@ def run_mixed(args, dist: Dist) -> dict:
 
 
 def run_profile_case(args):
-    """One insert + one stream query of a small case (genome scale 0.1: 200 MB of reads, 2 GiB
-    table) with the chosen strategy: the command the ncu captures profile."""
+    """One insert + one stream query with the chosen strategy, on the 2 GiB table: genome scale
+    0.1 (200 MB of reads) for multi-pass ncu captures, scale 1.0 (the full 2 Gbp) for one-pass
+    DRAM-byte captures."""
     import torch
 
     from scbf_b200 import _lib, api
 
     L = _lib.load()
-    data, offsets = workload(0, 0.1)
+    data, offsets = workload(0, args.profile_scale)
     cfg = api.SuperCountingBloomConfig(k=GEOM["k"], m=GEOM["m"], s=GEOM["s"], n_hashes=GEOM["n_hashes"],
                                        counter_bits=api.CounterBits(GEOM["counter_bits"]),
                                        counter_slots_exponent=GEOM["counter_slots_exponent"],

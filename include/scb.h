@@ -211,6 +211,19 @@ typedef struct scb_timings {
 scb_status scb_set_timing(scb_ctx* ctx, int enable); /* enabling also clears the totals */
 scb_status scb_get_timings(const scb_ctx* ctx, scb_timings* out);
 
+/* CUDA graphs per batch shape (no counterpart in the reference).  A batch of the fused or
+ * grouped strategy (scb_insert_batch[_device], scb_query_report[_device],
+ * scb_build_and_stream_query[_device]) replays a graph captured for its shape class: batch
+ * kind, byte capacity (the batch's bytes rounded up to four steps per octave, at least 64 KiB),
+ * sequence capacity (a power of two, at least 256) and strategies.  The batch's sizes and input
+ * pointers reach the kernels through a device parameter block, so one capture serves every
+ * batch of its class.  A replay whose super-k-mer records outgrow the class's record slots
+ * applies nothing and the batch is redone eagerly.  Results are identical either way.
+ * Default on; enable = 0 runs every batch eagerly (the plain strategy always does). */
+scb_status scb_set_graphs(scb_ctx* ctx, int enable);
+/* Graph captures, replays, and replays redone eagerly (record overflow or failed capture). */
+scb_status scb_graph_stats(const scb_ctx* ctx, uint64_t* captures, uint64_t* replays, uint64_t* fallbacks);
+
 /* ---------------------------------------------------------------------------------------
  * Serving: a request loop over a frozen, device-resident index (no counterpart in the
  * reference, whose queries run per call; this batches SuperCountingBloomIndex::
@@ -252,6 +265,9 @@ scb_status scb_server_submit(scb_server* s, const uint8_t* seqs, const uint64_t*
 scb_status scb_server_wait(scb_server* s, uint64_t ticket, scb_request_stats* stats);
 scb_status scb_server_get_summary(scb_server* s, scb_server_summary* out);
 scb_status scb_server_reset_stats(scb_server* s);
+/* Graphs captured (one per slot and shape class) and batches replayed through them.  A server
+ * uses graphs when its index context had them on at scb_server_create (scb_set_graphs). */
+scb_status scb_server_graph_stats(scb_server* s, uint64_t* captures, uint64_t* replays);
 /* Drains in-flight batches, then frees the server (not the index). */
 void scb_server_destroy(scb_server* s);
 

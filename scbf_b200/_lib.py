@@ -134,6 +134,8 @@ def load(path: str | None = None):
         "scb_debug_window_minimizers": (C.c_int, [ctxp, vp, vp, C.c_uint64, vp]),
         "scb_set_timing": (C.c_int, [ctxp, C.c_int]),
         "scb_get_timings": (C.c_int, [ctxp, C.POINTER(ScbTimings)]),
+        "scb_set_graphs": (C.c_int, [ctxp, C.c_int]),
+        "scb_graph_stats": (C.c_int, [ctxp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
         "scb_reset": (C.c_int, [ctxp]),
         "scb_query_report_device_noalloc": (C.c_int, [ctxp, vp, vp, C.c_uint64, C.c_uint64, vp,
                                                       C.POINTER(ScbReport)]),
@@ -142,6 +144,7 @@ def load(path: str | None = None):
         "scb_server_wait": (C.c_int, [vp, C.c_uint64, C.POINTER(ScbRequestStats)]),
         "scb_server_get_summary": (C.c_int, [vp, C.POINTER(ScbServerSummary)]),
         "scb_server_reset_stats": (C.c_int, [vp]),
+        "scb_server_graph_stats": (C.c_int, [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
         "scb_server_destroy": (None, [vp]),
         "scb_autotune": (C.c_int, [ctxp, vp, vp, C.c_uint64, C.POINTER(ScbTuning)]),
         "scb_get_tuning": (C.c_int, [ctxp, C.POINTER(ScbTuning)]),

@@ -61,6 +61,13 @@ __device__ __forceinline__ uint64_t revcomp(uint64_t v, uint32_t len) {
     return r ^ (0xAAAAAAAAAAAAAAAAull >> sh);
 }
 
+// Reverse complement of the 16 bases of one code word (base t moves to 15 - t).
+__device__ __forceinline__ uint32_t revcomp16(uint32_t w) {
+    uint32_t r = __brev(w);
+    r = ((r >> 1) & 0x55555555u) | ((r & 0x55555555u) << 1);
+    return r ^ 0xAAAAAAAAu;
+}
+
 __device__ __forceinline__ uint64_t canonical(uint64_t fwd, uint32_t len) {
     const uint64_t rc = revcomp(fwd, len);
     return fwd < rc ? fwd : rc;
@@ -186,9 +193,10 @@ template <int BITS>
 __device__ __forceinline__ uint32_t estimate_smer(const void* table, const DevGeom& g, uint64_t base, uint64_t smer) {
     uint64_t hash = xorshift64(smer);
     uint32_t est = CounterTraits<BITS>::kMax;
-    for (uint32_t i = 0; i < g.h; i++) {
+    for (uint32_t i = 1;; i++) {  // n_hashes >= 1; the chain's value after the last probe is unused
         const uint32_t v = load_counter<BITS>(table, base + (hash & g.bs_mask));
         est = v < est ? v : est;
+        if (i >= g.h) break;
         hash = xorshift64(hash);
     }
     return est;
@@ -199,8 +207,9 @@ template <int BITS>
 __device__ __forceinline__ void insert_smer(uint32_t* table32, const DevGeom& g, uint64_t base, uint64_t smer,
                                             uint32_t* status) {
     uint64_t hash = xorshift64(smer);
-    for (uint32_t i = 0; i < g.h; i++) {
+    for (uint32_t i = 1;; i++) {
         sat_inc<BITS>(table32, base + (hash & g.bs_mask), status);
+        if (i >= g.h) break;
         hash = xorshift64(hash);
     }
 }

@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "../../include/scb.h"
 #include "scb_kernels.cuh"
@@ -87,7 +88,6 @@ struct DevBuf {
 
 // Largest batch the kernels index with 32-bit positions.
 constexpr uint64_t kMaxBatchBytes = (1ull << 31);
-constexpr uint64_t kPadWords = 16;
 
 // Prepared grouped batch of a lane: sorted records and work items for the lane's current codes.
 struct GroupedState {
@@ -97,21 +97,71 @@ struct GroupedState {
     GroupArgs ga{};
 };
 
+// Timing events of a lane: which spans the current batch recorded (read_counters adds them up).
+enum TimedSpan : uint32_t {
+    kSpanPack = 1,          // ev 0 -> 1
+    kSpanInsert = 2,        // ev 2 -> 3
+    kSpanCut = 4,           // ev 4 -> 5 cut, 5 -> 6 bucketing
+    kSpanApplyInsert = 8,   // ev 7 -> 8
+    kSpanQuery = 16,        // ev 9 -> 10
+    kSpanApplyQuery = 32,   // ev 11 -> 12
+};
+constexpr int kLaneEvents = 13;
+
+// Byte class of a grouped graph: bytes rounded up to four steps per octave (at least 64 KiB).
+inline uint64_t class_bytes(uint64_t n) {
+    if (n <= (64u << 10)) return 64u << 10;
+    const uint32_t e = 63u - (uint32_t)__builtin_clzll(n - 1);  // 2^e <= n - 1 < 2^(e + 1)
+    const uint64_t step = 1ull << (e - 2);
+    return ((n + step - 1) / step) * step;
+}
+
+// Kinds of batch a lane runs, eagerly or as a replay of a captured graph.
+enum BatchKind : int { kBatchInsert = 1, kBatchReport = 2, kBatchBuildStream = 3 };
+
+// Shape class of a graph: batch kind, strategies, byte capacity and the grouped pipeline's
+// sizes, plus a signature of the lane buffers the graph's nodes point at.
+struct GraphKey {
+    int kind = 0, s_ins = 0, s_query = 0;
+    uint64_t cap_bytes = 0, rec_cap = 0, max_items = 0, n_buckets = 0;
+    uint32_t shift = 0, apply_threads = 0;
+    uint64_t sig = 0;
+    bool operator==(const GraphKey& o) const {
+        return kind == o.kind && s_ins == o.s_ins && s_query == o.s_query &&
+               cap_bytes == o.cap_bytes && rec_cap == o.rec_cap &&
+               max_items == o.max_items && n_buckets == o.n_buckets && shift == o.shift &&
+               apply_threads == o.apply_threads && sig == o.sig;
+    }
+};
+
+struct GraphEntry {
+    GraphKey key;
+    cudaGraphExec_t exec = nullptr;
+    uint64_t launches = 0;  // kernels per replay
+    uint64_t last_use = 0;
+};
+
 // Derived per-batch arrays (codes, bitmaps, window offsets, plain-pipeline arrays, counters).
 struct Lane {
-    DevBuf ascii, offsets, codes, valid, seqstart, woff, scan, wblock, wend, cnt, tiles;
+    DevBuf ascii, offsets, codes, valid, seqstart, woff, scan, wblock, wend, cnt, cnt2, tiles, params;
     // grouped pipeline: records, bucket offsets / cursors, work items
     DevBuf rec_key, rec_val, rec_sorted, bhist, bcursor, icount, items, gscan, rec_count;
     cudaStream_t stream = nullptr;
     GroupedState gs;
-    // stage timing: [0,1] pack, [2,3] main stage (main_kind 1 = insert, 2 = query),
-    // [4,5,6] grouped cut start / cut end / prepare end, [7,8] apply start / end
-    cudaEvent_t ev[9] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
-    bool pack_timed = false;
-    bool cut_timed = false;
-    int main_kind = 0;
-    int grouped_kind = 0;
+    cudaEvent_t ev[kLaneEvents] = {};
+    uint32_t spans = 0;
+    // captured graphs of this lane by shape class, the pinned parameter block their first node
+    // copies to the device, and the record capacity learned from overflowing replays
+    std::vector<GraphEntry> graphs;
+    BatchParams* h_params = nullptr;
+    uint64_t rec_hint = 0;
+    bool recording = false;  // a stream capture of this lane is in progress
+    uint64_t graph_clock = 0, captures = 0, replays = 0, graph_fallbacks = 0;
     ~Lane() {
+        for (auto& g : graphs) {
+            if (g.exec) cudaGraphExecDestroy(g.exec);
+        }
+        if (h_params) cudaFreeHost(h_params);
         for (auto& e : ev) {
             if (e) cudaEventDestroy(e);
         }
@@ -150,6 +200,7 @@ struct scb_ctx {
     scb::Tuning tuning;
     scb::Lane lane;
     bool timing = false;
+    bool graphs = true;  // replay batches through graphs captured per shape class
     scb_timings times{};
     std::mutex mu;
     ~scb_ctx() {

@@ -30,7 +30,17 @@ namespace {
 std::atomic<uint64_t> g_launches{0};
 }
 
-void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+// While a thread records a graph, its launches are counted into the graph (run at each replay).
+thread_local uint64_t* t_recording = nullptr;
+void note_launch() {
+    if (t_recording) {
+        ++*t_recording;
+    } else {
+        g_launches.fetch_add(1, std::memory_order_relaxed);
+    }
+}
+void note_launches(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+void record_launches_into(uint64_t* counter) { t_recording = counter; }
 uint64_t kernel_launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
 // ---------------------------------------------------------------------------------------
@@ -86,16 +96,29 @@ __global__ void k_pack(const uint8_t* __restrict__ ascii, uint64_t n, uint32_t* 
     }
 }
 
-// Graph-replayable packing: the batch's byte count comes from device memory (params[0]); the
-// launch covers the capacity of its shape class, groups past the batch write empty words.
-__global__ void k_pack_dyn(const uint8_t* __restrict__ ascii, const uint64_t* __restrict__ params,
-                           uint32_t* __restrict__ codes, uint32_t* __restrict__ valid, uint64_t cap_groups) {
-    const uint64_t n = params[0];
+// Graph-replayable kernels.  The batch's sizes and inputs come from the device parameter block
+// and every launch has a fixed grid (grid-stride loops), so a captured graph serves batches of any
+// size that fit its buffers.
+
+// Packing: groups [0, groups(n)) from the reads, then kPadWords zero words after the batch in
+// both arrays (the padding the tile kernels may read).
+__global__ void k_pack_dyn(const BatchParams* __restrict__ bp, uint32_t* __restrict__ codes,
+                           uint32_t* __restrict__ valid) {
+    const uint64_t n = bp->n_bytes;
+    const uint64_t n_groups = (n + 31) / 32;
+    const uint8_t* __restrict__ ascii = bp->ascii;
+    const bool aligned = (reinterpret_cast<uintptr_t>(ascii) & 15u) == 0;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t gi = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; gi < cap_groups; gi += stride) {
+    for (uint64_t gi = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; gi < n_groups + kPadWords; gi += stride) {
+        if (gi >= n_groups) {
+            const uint64_t t = gi - n_groups;
+            valid[n_groups + t] = 0;
+            codes[2 * n_groups + t] = 0;
+            continue;
+        }
         const uint64_t base = gi * 32;
         uint32_t w[8];
-        if (base + 32 <= n) {
+        if (aligned && base + 32 <= n) {
             const uint4 x = __ldcs(reinterpret_cast<const uint4*>(ascii + base));
             const uint4 y = __ldcs(reinterpret_cast<const uint4*>(ascii + base + 16));
             w[0] = x.x; w[1] = x.y; w[2] = x.z; w[3] = x.w;
@@ -129,10 +152,25 @@ __global__ void k_pack_dyn(const uint8_t* __restrict__ ascii, const uint64_t* __
     }
 }
 
-// Graph-replayable sequence starts: the sequence count comes from device memory (params[1]).
-__global__ void k_seqstart_dyn(const uint64_t* __restrict__ offsets, const uint64_t* __restrict__ params,
-                               uint32_t* __restrict__ seqstart) {
-    const uint64_t n_bytes = params[0], n_seqs = params[1];
+// Clears the sequence-start bitmap of the batch and, when given, its per-window outputs (at most
+// one window per byte).
+__global__ void k_clear_dyn(const BatchParams* __restrict__ bp, uint32_t* __restrict__ seqstart,
+                            unsigned long long* __restrict__ out, uint8_t* __restrict__ out_valid) {
+    const uint64_t n = bp->n_bytes;
+    const uint64_t n_words = (n + 31) / 32 + kPadWords;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t t0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (uint64_t i = t0; i < n_words; i += stride) seqstart[i] = 0;
+    if (out) {
+        for (uint64_t i = t0; i < n; i += stride) out[i] = 0;
+        for (uint64_t i = t0; i < (n + 15) / 16; i += stride) reinterpret_cast<uint4*>(out_valid)[i] = make_uint4(0, 0, 0, 0);
+    }
+}
+
+// Sequence starts (after k_clear_dyn).
+__global__ void k_seqstart_dyn(const BatchParams* __restrict__ bp, uint32_t* __restrict__ seqstart) {
+    const uint64_t n_bytes = bp->n_bytes, n_seqs = bp->n_seqs;
+    const uint64_t* __restrict__ offsets = bp->offsets;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n_seqs; j += stride) {
         const uint64_t a = offsets[j], b = offsets[j + 1];
@@ -140,21 +178,44 @@ __global__ void k_seqstart_dyn(const uint64_t* __restrict__ offsets, const uint6
     }
 }
 
-void launch_pack_dyn(const uint8_t* ascii, const uint64_t* params, uint64_t cap_bytes, uint32_t* codes,
-                     uint32_t* valid, cudaStream_t st) {
-    const uint64_t groups = (cap_bytes + 31) / 32;
-    if (groups == 0) return;
-    const uint64_t blocks = (groups + 255) / 256;
-    k_pack_dyn<<<(unsigned)(blocks < (1u << 20) ? blocks : (1u << 20)), 256, 0, st>>>(ascii, params, codes, valid,
-                                                                                      groups);
+// Window and record counts (the QueryFastaReport totals).
+__global__ void k_seq_windows_dyn(const BatchParams* __restrict__ bp, uint32_t k, unsigned long long* cnt) {
+    const uint64_t n_seqs = bp->n_seqs;
+    const uint64_t* __restrict__ offsets = bp->offsets;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    unsigned long long total = 0, recs = 0;
+    const uint64_t n_iter = (n_seqs + stride - 1) / stride;
+    for (uint64_t it = 0; it < n_iter; it++) {
+        const uint64_t j = it * stride + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+        if (j < n_seqs) {
+            const uint64_t len = offsets[j + 1] - offsets[j];
+            total += len >= k ? len + 1 - k : 0;
+            recs += 1;
+        }
+    }
+    warp_add_u64(&cnt[kCntTotalWindows], total);
+    warp_add_u64(&cnt[kCntRecords], recs);
+}
+
+void launch_pack_dyn(const BatchParams* bp, uint32_t* codes, uint32_t* valid, int sm_count, cudaStream_t st) {
+    k_pack_dyn<<<(unsigned)(sm_count * 8), 256, 0, st>>>(bp, codes, valid);
     note_launch();
 }
 
-void launch_seqstart_dyn(const uint64_t* offsets, const uint64_t* params, uint64_t cap_seqs, uint32_t* seqstart,
-                         cudaStream_t st) {
-    if (cap_seqs == 0) return;
-    const uint64_t blocks = (cap_seqs + 255) / 256;
-    k_seqstart_dyn<<<(unsigned)(blocks < 65536 ? blocks : 65536), 256, 0, st>>>(offsets, params, seqstart);
+void launch_clear_dyn(const BatchParams* bp, uint32_t* seqstart, unsigned long long* out, uint8_t* out_valid,
+                      int sm_count, cudaStream_t st) {
+    k_clear_dyn<<<(unsigned)(sm_count * 4), 256, 0, st>>>(bp, seqstart, out, out_valid);
+    note_launch();
+}
+
+void launch_seqstart_dyn(const BatchParams* bp, uint32_t* seqstart, int sm_count, cudaStream_t st) {
+    k_seqstart_dyn<<<(unsigned)(sm_count * 2), 256, 0, st>>>(bp, seqstart);
+    note_launch();
+}
+
+void launch_seq_windows_dyn(const BatchParams* bp, uint32_t k, unsigned long long* cnt, int sm_count,
+                            cudaStream_t st) {
+    k_seq_windows_dyn<<<(unsigned)(sm_count * 2), 256, 0, st>>>(bp, k, cnt);
     note_launch();
 }
 
@@ -413,6 +474,18 @@ __global__ void __launch_bounds__(kTileThreads, 8) k_tiles(TileArgs a) {
     // modes that read a block id for every valid window (the cut computes it at ends only)
     constexpr bool kBlockPerWindow = MODE == kModeInsert || MODE == kModeReport || MODE == kModeAbund ||
                                      MODE == kModeDistinct || MODE == kModeMaterialize;
+    // batch sizes: from the parameter block on graph replays, else from the arguments
+    uint64_t n_bytes = a.n_bytes, n_seqs = a.n_seqs, n_code_words = a.n_code_words, n_bit_words = a.n_bit_words;
+    uint32_t n_tiles = a.n_tiles;
+    const uint64_t* offsets = a.offsets;
+    if (a.dyn) {
+        n_bytes = a.dyn->n_bytes;
+        n_seqs = a.dyn->n_seqs;
+        offsets = a.dyn->offsets;
+        n_bit_words = (n_bytes + 31) / 32;
+        n_code_words = 2 * n_bit_words;
+        n_tiles = (uint32_t)((n_bytes + kTileWindows - 1) / kTileWindows);
+    }
     fill_nt_tables(sm, g.m);
     if (MODE == kModeCut && tid == 0) {
         sm.chunk_base = 0;
@@ -424,7 +497,7 @@ __global__ void __launch_bounds__(kTileThreads, 8) k_tiles(TileArgs a) {
         if (tid == 0) sm.tile = atomicAdd(a.tile_counter, 1u);
         __syncthreads();
         const uint32_t tile = sm.tile;
-        if (tile >= a.n_tiles) break;
+        if (tile >= n_tiles) break;
         const uint64_t t0 = (uint64_t)tile * kTileWindows;
         const uint32_t back = (MODE == kModeStats || MODE == kModeCut)
                                   ? (uint32_t)(t0 < (uint64_t)kBack ? t0 : (uint64_t)kBack)
@@ -438,20 +511,20 @@ __global__ void __launch_bounds__(kTileThreads, 8) k_tiles(TileArgs a) {
         const uint64_t cw0 = cb >> 4;
         const uint32_t n_cw = (uint32_t)((e0 + n_eval + 96 - cb) >> 4) + 3;
         for (uint32_t i = tid; i < n_cw; i += blockDim.x) {
-            sm.codes[i] = (cw0 + i < a.n_code_words) ? __ldg(a.codes + cw0 + i) : 0u;
+            sm.codes[i] = (cw0 + i < n_code_words) ? __ldg(a.codes + cw0 + i) : 0u;
         }
         const uint64_t bb = e0 & ~31ull;
         const uint64_t bw0 = bb >> 5;
         const uint32_t n_bw = (uint32_t)((e0 + n_eval + 128 - bb) >> 5) + 3;
         for (uint32_t i = tid; i < n_bw; i += blockDim.x) {
-            const bool in = bw0 + i < a.n_bit_words;
+            const bool in = bw0 + i < n_bit_words;
             sm.valid[i] = in ? __ldg(a.valid + bw0 + i) : 0u;
             sm.start[i] = in ? __ldg(a.seqstart + bw0 + i) : 0u;
         }
         if (MODE == kModeAbund && tid == 0) {
-            sm.seq_lo = seq_of(a.offsets, 0, a.n_seqs, t0);
+            sm.seq_lo = seq_of(offsets, 0, n_seqs, t0);
             const uint64_t last = t0 + kTileWindows;
-            sm.seq_hi = seq_of(a.offsets, sm.seq_lo, a.n_seqs, last);
+            sm.seq_hi = seq_of(offsets, sm.seq_lo, n_seqs, last);
         }
         if (tid == 0) sm.n_ends = 0;
         __syncthreads();
@@ -559,8 +632,8 @@ __global__ void __launch_bounds__(kTileThreads, 8) k_tiles(TileArgs a) {
                     c_pos += r > 0;
                     c_sum += r;
                 } else if constexpr (MODE == kModeAbund) {
-                    const uint64_t j = seq_of(a.offsets, sm.seq_lo, sm.seq_hi, pos);
-                    const uint64_t o = a.woff[j] + (pos - __ldg(a.offsets + j));
+                    const uint64_t j = seq_of(offsets, sm.seq_lo, sm.seq_hi, pos);
+                    const uint64_t o = a.woff[j] + (pos - __ldg(offsets + j));
                     a.out[o] = r;
                     a.out_valid[o] = 1;
                 } else {
@@ -601,9 +674,10 @@ __global__ void __launch_bounds__(kTileThreads, 8) k_tiles(TileArgs a) {
                     for (uint32_t q = 0; q < n_sm; q++) {
                         const uint64_t smer = canonical(codes64(sm.codes, e0 + st + q - cb) & s_mask, g.s);
                         uint64_t hash = xorshift64(smer);
-                        for (uint32_t h = 0; h < g.h; h++) {
+                        for (uint32_t h = 1;; h++) {
                             const uint32_t sec = (uint32_t)(((hash & g.bs_mask) * bytes_per) >> 5);
                             seen[sec >> 5] |= 1u << (sec & 31);
+                            if (h >= g.h) break;
                             hash = xorshift64(hash);
                         }
                     }
@@ -689,12 +763,12 @@ __global__ void __launch_bounds__(kTileThreads, 8) k_tiles(TileArgs a) {
         } else if constexpr (MODE == kModeDebugMin) {
             for (uint32_t i = tid; i < kTileWindows; i += blockDim.x) {
                 const uint64_t pos = t0 + i;
-                if (sm.poff[i] != kNoWindow && pos < a.n_bytes) a.dbg[pos] = (uint32_t)(e0 + sm.poff[i]);
+                if (sm.poff[i] != kNoWindow && pos < n_bytes) a.dbg[pos] = (uint32_t)(e0 + sm.poff[i]);
             }
         } else if constexpr (MODE == kModeMaterialize) {
             for (uint32_t i = tid; i < kTileWindows; i += blockDim.x) {
                 const uint64_t pos = t0 + i;
-                if (pos >= a.n_bytes) continue;
+                if (pos >= n_bytes) continue;
                 const uint16_t po = sm.poff[i];
                 a.wblock[pos] = po == kNoWindow ? 0xFFFFFFFFu : sm.block[i];
                 a.wend[pos] = (po != kNoWindow && sm.poff[i + 1] != po) ? 1 : 0;
@@ -933,7 +1007,8 @@ void launch_counter_hist(const void* table, uint64_t slots, int bits, unsigned l
 __global__ void k_scatter(const uint32_t* __restrict__ key, const unsigned long long* __restrict__ val,
                           const unsigned long long* __restrict__ count, uint64_t cap, uint32_t shift,
                           unsigned long long* __restrict__ cursor, unsigned long long* __restrict__ sorted) {
-    const uint64_t n = min((uint64_t)*count, cap);
+    const uint64_t n = *count;
+    if (n > cap) return;  // the cut ran out of record slots: the host redoes the batch
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     const uint32_t local_mask = (1u << shift) - 1u;
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
@@ -946,10 +1021,12 @@ __global__ void k_scatter(const uint32_t* __restrict__ key, const unsigned long 
 }
 
 __global__ void k_item_counts(const unsigned long long* __restrict__ off, uint64_t n_buckets,
-                              uint64_t* __restrict__ item_count) {
+                              uint64_t* __restrict__ item_count, const unsigned long long* __restrict__ rec_count,
+                              uint64_t rec_cap) {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const bool overflow = *rec_count > rec_cap;  // no work items: nothing is applied
     for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; b <= n_buckets; b += stride) {
-        if (b == n_buckets) {
+        if (b == n_buckets || overflow) {
             item_count[b] = 0;
         } else {
             const uint64_t c = off[b + 1] - off[b];
@@ -1048,11 +1125,13 @@ struct CounterType<16> {
 //   rv      the chunk's records
 //   spre    exclusive prefix of s-mers per record, wpre the same for windows
 //   bases   the 2-bit code words of each record of the chunk
+//   rbases  the same words reverse-complemented (word j = revcomp of word 7 - j), plus spare
+//           words that the last record's reads may touch
 //   smap    record of each s-mer of the chunk, wmap record of each window (query)
 //   touched one flag per block of the bucket
 //   est     s-mer minima of the chunk (query; 16-bit for 8/16-bit counters)
 struct ApplyLayout {
-    uint32_t cells, rv, spre, wpre, bases, smap, wmap, touched, est, total;
+    uint32_t cells, rv, spre, wpre, bases, rbases, smap, wmap, touched, est, total;
 };
 
 // s-mers (and windows) of one staged chunk of records; a record has at most 31 + 31
@@ -1072,7 +1151,8 @@ __host__ __device__ inline ApplyLayout apply_layout(int mode, int bits, uint32_t
     l.spre = l.rv + align16(kApplyChunk * 8u);
     l.wpre = l.spre + align16((kApplyChunk + 1u) * 4u);
     l.bases = l.wpre + align16((kApplyChunk + 1u) * 4u);
-    l.smap = l.bases + kApplyChunk * kRecBaseWords * 4u;
+    l.rbases = l.bases + kApplyChunk * kRecBaseWords * 4u;
+    l.smap = l.rbases + kApplyChunk * kRecBaseWords * 4u + 16u;
     l.wmap = l.smap + align16(max_smers);
     l.touched = l.wmap + (mode == kModeInsert ? 0u : align16(max_windows));
     l.est = l.touched + align16(bucket_blocks);
@@ -1096,6 +1176,7 @@ __global__ void __launch_bounds__(kApplyMaxThreads) k_apply(GroupArgs a, uint32_
     uint32_t* spre = reinterpret_cast<uint32_t*>(smem_raw + lay.spre);
     uint32_t* wpre = reinterpret_cast<uint32_t*>(smem_raw + lay.wpre);
     uint32_t* bases = reinterpret_cast<uint32_t*>(smem_raw + lay.bases);
+    uint32_t* rbases = reinterpret_cast<uint32_t*>(smem_raw + lay.rbases);
     uint8_t* smap = smem_raw + lay.smap;
     uint8_t* wmap = smem_raw + lay.wmap;
     uint8_t* touched = smem_raw + lay.touched;
@@ -1108,6 +1189,7 @@ __global__ void __launch_bounds__(kApplyMaxThreads) k_apply(GroupArgs a, uint32_
     const uint64_t s_mask = len_mask(g.s);
     uint32_t* table32 = reinterpret_cast<uint32_t*>(a.table);
     const uint64_t n_items = *a.n_items;
+    if (a.rec_count && *a.rec_count > a.rec_cap) return;  // records outgrew their slots: host redoes it
     unsigned long long c_valid = 0, c_pos = 0, c_sum = 0;
 
     while (true) {
@@ -1148,12 +1230,15 @@ __global__ void __launch_bounds__(kApplyMaxThreads) k_apply(GroupArgs a, uint32_
             chunk_prefix(rv, nrec, ks, spre, wpre, warp_tot);
             // the leading records whose s-mers fit the chunk's budget (at least one)
             const uint32_t nuse = (uint32_t)__syncthreads_count(tid < nrec && spre[tid + 1] <= kSmerBudget);
-            if (tid < nuse) {  // stage the record's bases; record index of its s-mers / windows
-                const unsigned long long v = rv[tid];
-                const uint64_t w0 = (uint32_t)v >> 4;
-                uint32_t* rb = bases + tid * kRecBaseWords;
-#pragma unroll
-                for (uint32_t x = 0; x < kRecBaseWords; x++) rb[x] = __ldg(a.codes + w0 + x);
+            // stage the records' bases, kRecBaseWords consecutive threads per record (one sector
+            // read, conflict-free shared stores), and their reverse complements
+            for (uint32_t x = tid; x < nuse * kRecBaseWords; x += blockDim.x) {
+                const uint32_t r = x / kRecBaseWords, j = x % kRecBaseWords;
+                const uint32_t cw = __ldg(a.codes + ((uint32_t)rv[r] >> 4) + j);
+                bases[x] = cw;
+                rbases[r * kRecBaseWords + (kRecBaseWords - 1 - j)] = revcomp16(cw);
+            }
+            if (tid < nuse) {  // record index of its s-mers / windows
                 const uint32_t s0 = spre[tid], s1 = spre[tid + 1];
                 for (uint32_t f = s0; f < s1; f++) smap[f] = (uint8_t)tid;
                 if constexpr (MODE == kModeReport) {
@@ -1170,20 +1255,27 @@ __global__ void __launch_bounds__(kApplyMaxThreads) k_apply(GroupArgs a, uint32_
                 const uint32_t start = (uint32_t)v;
                 const uint32_t rel = (start & 15u) + (f - spre[r]);  // base offset in the staged words
                 const uint32_t lb = (uint32_t)(v >> kRecLocalShift);
-                const uint64_t smer = canonical(codes64(bases + r * kRecBaseWords, rel) & s_mask, g.s);
-                uint64_t hash = xorshift64(smer);
+                // forward s-mer from the staged words; its reverse complement from the mirrored
+                // words: base t of it is the complement of forward base rel + s - 1 - t, which
+                // sits at position 16 * kRecBaseWords - rel - s + t of the mirrored stream (bits
+                // read past the record's words land above 2s and are masked off)
+                const uint64_t fw = codes64(bases + r * kRecBaseWords, rel) & s_mask;
+                const uint64_t rc = codes64(rbases + r * kRecBaseWords, 16u * kRecBaseWords - rel - g.s) & s_mask;
+                uint64_t hash = xorshift64(fw < rc ? fw : rc);
                 Cell* blk = cells + (lb << bs_log2);
                 if constexpr (MODE == kModeInsert) {
-                    for (uint32_t h = 0; h < g.h; h++) {
+                    for (uint32_t h = 1;; h++) {  // n_hashes >= 1; no mix after the last probe
                         atomicAdd(blk + (hash & g.bs_mask), 1u);
+                        if (h >= g.h) break;
                         hash = xorshift64(hash);
                     }
                     touched[lb] = 1;
                 } else {
                     uint32_t e = T::kMax;
-                    for (uint32_t h = 0; h < g.h; h++) {
+                    for (uint32_t h = 1;; h++) {
                         const uint32_t c = blk[hash & g.bs_mask];
                         e = c < e ? c : e;
+                        if (h >= g.h) break;
                         hash = xorshift64(hash);
                     }
                     est[f] = (Est)e;
@@ -1293,9 +1385,10 @@ void launch_scatter(const uint32_t* rec_key, const unsigned long long* rec_val, 
 }
 
 void launch_item_counts(const unsigned long long* bucket_off, uint64_t n_buckets, uint64_t* item_count,
-                        cudaStream_t st) {
+                        const unsigned long long* rec_count, uint64_t rec_cap, cudaStream_t st) {
     const uint64_t blocks = (n_buckets + 1 + 255) / 256;
-    k_item_counts<<<(unsigned)(blocks < 16384 ? blocks : 16384), 256, 0, st>>>(bucket_off, n_buckets, item_count);
+    k_item_counts<<<(unsigned)(blocks < 16384 ? blocks : 16384), 256, 0, st>>>(bucket_off, n_buckets, item_count,
+                                                                              rec_count, rec_cap);
     note_launch();
 }
 

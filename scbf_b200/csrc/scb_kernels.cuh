@@ -9,6 +9,9 @@
 
 namespace scb {
 
+// Zero words kept after a batch's codes and bitmaps (reads that run past the last base).
+constexpr uint64_t kPadWords = 16;
+
 // Tile geometry of the fused kernels: windows per tile and threads per CTA.
 constexpr int kTileWindows = 1024;
 constexpr int kTileThreads = 256;
@@ -23,6 +26,15 @@ enum TileMode : int {
     kModeMaterialize = 6,  // (b) for the plain pipeline: per-window block id + end flag in HBM
     kModeInsertStaged = 7, // (b)+(c)+(d) with one warp per super-k-mer staging block deltas
     kModeCut = 8           // (b) for the grouped pipeline: one record per super-k-mer + bucket counts
+};
+
+// Sizes and input pointers of one batch, in device memory: a graph captured for a shape class
+// reads them at replay, so one graph serves every batch of its class.
+struct BatchParams {
+    uint64_t n_bytes;
+    uint64_t n_seqs;
+    const uint8_t* ascii;
+    const uint64_t* offsets;
 };
 
 // Grouped pipeline: super-k-mer records bucketed by counter block.
@@ -48,6 +60,11 @@ struct GroupArgs {
     unsigned int* work_counter;
     uint32_t bucket_shift;
     uint32_t apply_threads;  // CTA width of the apply kernel: 128, 256 (default) or 512
+    // record slots the cut reserved and the capacity it had: when the count exceeds the capacity
+    // (a graph replay whose records outgrew its class) the apply does nothing and the host redoes
+    // the batch with room for every record
+    const unsigned long long* rec_count;
+    uint64_t rec_cap;
 };
 
 // Slots of the per-launch 64-bit counter array.
@@ -106,15 +123,23 @@ struct TileArgs {
     unsigned long long* bucket_hist;
     uint32_t bucket_shift;
     uint32_t pad3_;
+    // when set, n_bytes / n_seqs / offsets come from here at run time (graph replays) and the
+    // fields above give the capacity of the batch's shape class
+    const BatchParams* dyn;
 };
 
 // Kernel launches; each counts itself in the library-wide launch counter.
 void launch_pack(const uint8_t* ascii, uint64_t n_bytes, uint32_t* codes, uint32_t* valid, cudaStream_t st);
-// graph-replayable forms: sizes read from params[0] (bytes) / params[1] (sequences) on the device
-void launch_pack_dyn(const uint8_t* ascii, const uint64_t* params, uint64_t cap_bytes, uint32_t* codes,
-                     uint32_t* valid, cudaStream_t st);
-void launch_seqstart_dyn(const uint64_t* offsets, const uint64_t* params, uint64_t cap_seqs, uint32_t* seqstart,
-                         cudaStream_t st);
+// Graph-replayable forms: the batch's sizes and input pointers come from a BatchParams block in
+// device memory; grids are fixed (grid-stride loops over the batch), so one capture serves any
+// batch that fits the buffers.  The out / out_valid buffers of launch_clear_dyn need 16-byte
+// alignment and room for n_bytes rounded up to 16.
+void launch_pack_dyn(const BatchParams* bp, uint32_t* codes, uint32_t* valid, int sm_count, cudaStream_t st);
+void launch_clear_dyn(const BatchParams* bp, uint32_t* seqstart, unsigned long long* out, uint8_t* out_valid,
+                      int sm_count, cudaStream_t st);
+void launch_seqstart_dyn(const BatchParams* bp, uint32_t* seqstart, int sm_count, cudaStream_t st);
+void launch_seq_windows_dyn(const BatchParams* bp, uint32_t k, unsigned long long* cnt, int sm_count,
+                            cudaStream_t st);
 void launch_seqstart(const uint64_t* offsets, uint64_t n_seqs, uint64_t n_bytes, uint32_t* seqstart,
                      cudaStream_t st);
 void launch_seq_windows(const uint64_t* offsets, uint64_t n_seqs, uint32_t k, unsigned long long* cnt,
@@ -132,7 +157,7 @@ void launch_scatter(const uint32_t* rec_key, const unsigned long long* rec_val, 
                     uint64_t rec_cap, uint32_t bucket_shift, unsigned long long* cursor, unsigned long long* sorted,
                     cudaStream_t st);
 void launch_item_counts(const unsigned long long* bucket_off, uint64_t n_buckets, uint64_t* item_count,
-                        cudaStream_t st);
+                        const unsigned long long* rec_count, uint64_t rec_cap, cudaStream_t st);
 void launch_item_write(const unsigned long long* bucket_off, const uint64_t* item_off, uint64_t n_buckets,
                        uint4* items, cudaStream_t st);
 void launch_apply(int mode, const GroupArgs& a, int block_slots, uint32_t bucket_blocks, int sm_count,
@@ -140,5 +165,8 @@ void launch_apply(int mode, const GroupArgs& a, int block_slots, uint32_t bucket
 
 uint64_t kernel_launch_count();
 void note_launch();
+void note_launches(uint64_t n);  // kernels of one graph replay
+// Counts this thread's launches into *counter instead (a graph being recorded); nullptr ends it.
+void record_launches_into(uint64_t* counter);
 
 }  // namespace scb

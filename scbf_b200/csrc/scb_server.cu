@@ -6,7 +6,11 @@
 // all slots together fit the configured device-memory budget (admission control).  Whenever a
 // slot is free and pieces are pending, the scheduler packs the oldest pieces into a batch and
 // launches it on the slot's stream: H2D copy, 2-bit packing, the fused per-window abundance
-// kernel, D2H copy.  Batches of different slots overlap on the GPU; requests that arrive while
+// kernel, D2H copy.  The device work of a batch (clears, packing, sequence starts, abundance
+// kernel) is one replay of a CUDA graph captured once per slot: the batch's sizes reach the
+// kernels through a parameter block that the graph copies from the slot's pinned memory, and the
+// kernels' grids do not depend on the batch, so the same graph serves every batch shape.
+// Batches of different slots overlap on the GPU; requests that arrive while
 // others run are admitted as soon as a slot frees.  A host callback at the end of each batch
 // wakes the scheduler, which scatters the results into the requests' output buffers and
 // completes the requests whose pieces are all done.
@@ -58,7 +62,10 @@ struct Piece {
 
 struct Slot {
     cudaStream_t stream = nullptr;
-    DevBuf ascii, offsets, woff, codes, valid, seqstart, out, outv, cnt, tiles;
+    DevBuf ascii, offsets, woff, codes, valid, seqstart, out, outv, cnt, tiles, params;
+    BatchParams* h_params = nullptr;
+    cudaGraphExec_t graph = nullptr;  // the slot's batch, captured at its first batch
+    uint64_t graph_launches = 0;
     uint8_t* h_ascii = nullptr;
     uint64_t* h_offsets = nullptr;
     uint64_t* h_woff = nullptr;
@@ -69,6 +76,8 @@ struct Slot {
     bool busy = false;
     std::atomic<bool> complete{false};
     ~Slot() {
+        if (graph) cudaGraphExecDestroy(graph);
+        if (h_params) cudaFreeHost(h_params);
         if (h_ascii) cudaFreeHost(h_ascii);
         if (h_offsets) cudaFreeHost(h_offsets);
         if (h_woff) cudaFreeHost(h_woff);
@@ -98,11 +107,15 @@ struct scb_server {
     // statistics since the last reset
     std::vector<double> latencies;
     uint64_t stat_windows = 0, stat_batches = 0;
+    bool use_graphs = true;
+    uint64_t captures = 0, replays = 0;
     Clock::time_point first_submit{}, last_finish{};
     bool have_first = false;
 
     void run();
     scb_status launch(Slot& s);
+    scb_status record(Slot& s, cudaStream_t st);
+    scb_status capture(Slot& s);
     void complete(Slot& s);
 };
 
@@ -119,6 +132,73 @@ void CUDART_CB on_batch_done(void* p) {
 }
 
 }  // namespace
+
+// Tile arguments of the abundance kernel over a slot's buffers (sizes of the batch, or of the
+// shape class when the kernel reads the batch's own sizes from the parameter block).
+static TileArgs tile_args(const scb_server& srv, const Slot& s, uint64_t bytes, uint64_t seqs) {
+    const scb_ctx* c = srv.ctx;
+    const uint64_t groups = (bytes + 31) / 32;
+    TileArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.g = c->g;
+    a.codes = s.codes.as<uint32_t>();
+    a.valid = s.valid.as<uint32_t>();
+    a.seqstart = s.seqstart.as<uint32_t>();
+    a.n_bytes = bytes;
+    a.n_code_words = 2 * groups;
+    a.n_bit_words = groups;
+    a.n_tiles = (uint32_t)((bytes + kTileWindows - 1) / kTileWindows);
+    a.table = c->table;
+    a.status = c->status;
+    a.cnt = s.cnt.as<unsigned long long>();
+    a.tile_counter = s.tiles.as<unsigned int>();
+    a.offsets = s.offsets.as<uint64_t>();
+    a.n_seqs = seqs;
+    a.woff = s.woff.as<uint64_t>();
+    a.out = s.out.as<unsigned long long>();
+    a.out_valid = s.outv.as<uint8_t>();
+    return a;
+}
+
+// The graph body of one slot batch: sizes from the slot's parameter block, fixed grids.
+scb_status scb_server::record(Slot& s, cudaStream_t st) {
+    const BatchParams* bp = s.params.as<BatchParams>();
+    const int sms = ctx->sm_count;
+    SCB_CUDA(cudaMemcpyAsync(s.params.p, s.h_params, sizeof(BatchParams), cudaMemcpyHostToDevice, st));
+    SCB_CUDA(cudaMemsetAsync(s.cnt.p, 0, kCntSlots * 8, st));
+    SCB_CUDA(cudaMemsetAsync(s.tiles.p, 0, 64, st));
+    launch_clear_dyn(bp, s.seqstart.as<uint32_t>(), s.out.as<unsigned long long>(), s.outv.as<uint8_t>(), sms, st);
+    launch_pack_dyn(bp, s.codes.as<uint32_t>(), s.valid.as<uint32_t>(), sms, st);
+    launch_seqstart_dyn(bp, s.seqstart.as<uint32_t>(), sms, st);
+    // capacities of the slot; the tile kernel reads the batch's sizes from bp
+    TileArgs a = tile_args(*this, s, cfg.max_batch_bytes, cfg.max_batch_seqs);
+    a.dyn = bp;
+    launch_tiles(kModeAbund, a, tile_grid(kModeAbund, ctx->g.bits, sms, a.n_tiles), st);
+    SCB_CUDA(cudaGetLastError());
+    return SCB_OK;
+}
+
+scb_status scb_server::capture(Slot& s) {
+    SCB_CUDA(cudaStreamBeginCapture(s.stream, cudaStreamCaptureModeRelaxed));
+    record_launches_into(&s.graph_launches);
+    const scb_status rs = record(s, s.stream);
+    record_launches_into(nullptr);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(s.stream, &graph);
+    if (rs != SCB_OK || e != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        if (rs != SCB_OK) return rs;
+        return fail_kind(SCB_ERR_INTERNAL_STATE, std::string("graph capture: ") + cudaGetErrorString(e));
+    }
+    const cudaError_t ei = cudaGraphInstantiate(&s.graph, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ei != cudaSuccess) {
+        s.graph = nullptr;
+        return fail_kind(SCB_ERR_INTERNAL_STATE, std::string("graph instantiate: ") + cudaGetErrorString(ei));
+    }
+    captures++;
+    return SCB_OK;
+}
 
 scb_status scb_server::launch(Slot& s) {
     scb_ctx* c = ctx;
@@ -144,39 +224,29 @@ scb_status scb_server::launch(Slot& s) {
     if (bytes) SCB_CUDA(cudaMemcpyAsync(s.ascii.p, s.h_ascii, bytes, cudaMemcpyHostToDevice, st));
     SCB_CUDA(cudaMemcpyAsync(s.offsets.p, s.h_offsets, (seqs + 1) * 8, cudaMemcpyHostToDevice, st));
     if (seqs) SCB_CUDA(cudaMemcpyAsync(s.woff.p, s.h_woff, seqs * 8, cudaMemcpyHostToDevice, st));
-    SCB_CUDA(cudaMemsetAsync(s.codes.p, 0, (2 * groups + kPadWords) * 4, st));
-    SCB_CUDA(cudaMemsetAsync(s.valid.p, 0, (groups + kPadWords) * 4, st));
-    SCB_CUDA(cudaMemsetAsync(s.seqstart.p, 0, (groups + kPadWords) * 4, st));
-    SCB_CUDA(cudaMemsetAsync(s.cnt.p, 0, kCntSlots * 8, st));
-    SCB_CUDA(cudaMemsetAsync(s.tiles.p, 0, 64, st));
-    if (wins) {
-        SCB_CUDA(cudaMemsetAsync(s.out.p, 0, wins * 8, st));
-        SCB_CUDA(cudaMemsetAsync(s.outv.p, 0, wins, st));
-    }
-    if (bytes) {
-        launch_pack(s.ascii.as<uint8_t>(), bytes, s.codes.as<uint32_t>(), s.valid.as<uint32_t>(), st);
-        launch_seqstart(s.offsets.as<uint64_t>(), seqs, bytes, s.seqstart.as<uint32_t>(), st);
-        TileArgs a;
-        std::memset(&a, 0, sizeof(a));
-        a.g = c->g;
-        a.codes = s.codes.as<uint32_t>();
-        a.valid = s.valid.as<uint32_t>();
-        a.seqstart = s.seqstart.as<uint32_t>();
-        a.n_bytes = bytes;
-        a.n_code_words = 2 * groups;
-        a.n_bit_words = groups;
-        a.n_tiles = (uint32_t)((bytes + kTileWindows - 1) / kTileWindows);
-        a.table = c->table;
-        a.status = c->status;
-        a.cnt = s.cnt.as<unsigned long long>();
-        a.tile_counter = s.tiles.as<unsigned int>();
-        a.offsets = s.offsets.as<uint64_t>();
-        a.n_seqs = seqs;
-        a.woff = s.woff.as<uint64_t>();
-        a.out = s.out.as<unsigned long long>();
-        a.out_valid = s.outv.as<uint8_t>();
-        launch_tiles(kModeAbund, a, tile_grid(kModeAbund, c->g.bits, c->sm_count, a.n_tiles), st);
-        SCB_CUDA(cudaGetLastError());
+    if (bytes && use_graphs) {
+        if (!s.graph) SCB_TRY(capture(s));
+        *s.h_params = BatchParams{bytes, seqs, s.ascii.as<uint8_t>(), s.offsets.as<uint64_t>()};
+        SCB_CUDA(cudaGraphLaunch(s.graph, st));
+        note_launches(s.graph_launches);
+        replays++;
+    } else {
+        SCB_CUDA(cudaMemsetAsync(s.codes.p, 0, (2 * groups + kPadWords) * 4, st));
+        SCB_CUDA(cudaMemsetAsync(s.valid.p, 0, (groups + kPadWords) * 4, st));
+        SCB_CUDA(cudaMemsetAsync(s.seqstart.p, 0, (groups + kPadWords) * 4, st));
+        SCB_CUDA(cudaMemsetAsync(s.cnt.p, 0, kCntSlots * 8, st));
+        SCB_CUDA(cudaMemsetAsync(s.tiles.p, 0, 64, st));
+        if (wins) {
+            SCB_CUDA(cudaMemsetAsync(s.out.p, 0, wins * 8, st));
+            SCB_CUDA(cudaMemsetAsync(s.outv.p, 0, wins, st));
+        }
+        if (bytes) {
+            launch_pack(s.ascii.as<uint8_t>(), bytes, s.codes.as<uint32_t>(), s.valid.as<uint32_t>(), st);
+            launch_seqstart(s.offsets.as<uint64_t>(), seqs, bytes, s.seqstart.as<uint32_t>(), st);
+            TileArgs a = tile_args(*this, s, bytes, seqs);
+            launch_tiles(kModeAbund, a, tile_grid(kModeAbund, c->g.bits, c->sm_count, a.n_tiles), st);
+            SCB_CUDA(cudaGetLastError());
+        }
     }
     if (wins) {
         SCB_CUDA(cudaMemcpyAsync(s.h_out, s.out.p, wins * 8, cudaMemcpyDeviceToHost, st));
@@ -300,6 +370,7 @@ scb_status scb_server_create(scb_ctx* ctx, const scb_server_config* cfg_in, scb_
     srv->ctx = ctx;
     srv->cfg = cfg;
     srv->cfg.max_inflight = (uint32_t)n_slots;
+    srv->use_graphs = ctx->graphs;
     for (uint64_t i = 0; i < n_slots; i++) {
         auto s = std::make_unique<Slot>();
         SCB_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
@@ -310,9 +381,11 @@ scb_status scb_server_create(scb_ctx* ctx, const scb_server_config* cfg_in, scb_
         SCB_TRY(s->valid.ensure((groups + kPadWords) * 4));
         SCB_TRY(s->seqstart.ensure((groups + kPadWords) * 4));
         SCB_TRY(s->out.ensure(std::max<uint64_t>(B, 1) * 8));
-        SCB_TRY(s->outv.ensure(std::max<uint64_t>(B, 1)));
+        SCB_TRY(s->outv.ensure(B + 16));  // cleared in 16-byte stores
         SCB_TRY(s->cnt.ensure(kCntSlots * 8));
         SCB_TRY(s->tiles.ensure(64));
+        SCB_TRY(s->params.ensure(sizeof(BatchParams)));
+        SCB_CUDA(cudaMallocHost((void**)&s->h_params, sizeof(BatchParams)));
         SCB_CUDA(cudaMallocHost((void**)&s->h_ascii, B + 64));
         SCB_CUDA(cudaMallocHost((void**)&s->h_offsets, (R + 1) * 8));
         SCB_CUDA(cudaMallocHost((void**)&s->h_woff, (R + 1) * 8));
@@ -427,6 +500,14 @@ scb_status scb_server_get_summary(scb_server* s, scb_server_summary* out) {
         out->mean_ms = sum / (double)v.size();
     }
     if (s->have_first) out->span_s = std::chrono::duration<double>(s->last_finish - s->first_submit).count();
+    return SCB_OK;
+}
+
+scb_status scb_server_graph_stats(scb_server* s, uint64_t* captures, uint64_t* replays) {
+    if (!s) return fail_kind(SCB_ERR_INTERNAL_STATE, "null server");
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (captures) *captures = s->captures;
+    if (replays) *replays = s->replays;
     return SCB_OK;
 }
 
