@@ -55,6 +55,8 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-mixed", action="store_true", help="skip the mixed-length (config 4) comparison")
     p.add_argument("--no-serve", action="store_true", help="skip the serving (config 5) measurement")
+    p.add_argument("--no-tune", action="store_true",
+                   help="skip the autotuner (untuned defaults: fixed settings for comparing kernel builds)")
     p.add_argument("--profile-case", choices=["plain", "fused", "grouped"], default=None,
                    help="run one insert + query of a small case (for ncu) and exit")
     p.add_argument("--profile-scale", type=float, default=0.1,
@@ -318,10 +320,14 @@ def run_ours(args, dist: Dist):
 
     # autotune on a sample of the workload (first 2 M reads) outside the timed region
     tune = _lib.ScbTuning()
-    n_tune = min(n_seqs, 2_000_000)
-    t_tune = time.perf_counter()
-    check(L.scb_autotune(h, data.ctypes.data, offsets.ctypes.data, n_tune, C.byref(tune)))
-    tuning = dict(tune.as_dict(), sample_reads=n_tune, seconds=time.perf_counter() - t_tune)
+    if args.no_tune:
+        check(L.scb_get_tuning(h, C.byref(tune)))
+        tuning = dict(tune.as_dict(), sample_reads=0, seconds=0.0)
+    else:
+        n_tune = min(n_seqs, 2_000_000)
+        t_tune = time.perf_counter()
+        check(L.scb_autotune(h, data.ctypes.data, offsets.ctypes.data, n_tune, C.byref(tune)))
+        tuning = dict(tune.as_dict(), sample_reads=n_tune, seconds=time.perf_counter() - t_tune)
 
     g0 = graph_stats(L, h)
     ms, info = timed("auto", args.steps)

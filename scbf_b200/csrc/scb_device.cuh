@@ -74,10 +74,11 @@ __device__ __forceinline__ uint64_t canonical(uint64_t fwd, uint32_t len) {
 }
 
 // 64 bits of a 2-bit code stream starting at base b (words of 16 bases).  Reads words
-// b/16 .. b/16+2, which the caller keeps in bounds.
-__device__ __forceinline__ uint64_t codes64(const uint32_t* words, uint64_t b) {
-    const uint64_t w = b >> 4;
-    const uint32_t sh = (uint32_t)(b & 15) * 2u;
+// b/16 .. b/16+2, which the caller keeps in bounds.  Positions are below 2^31 (a batch's bases
+// or a tile's shared-memory stream), so the index arithmetic stays 32-bit.
+__device__ __forceinline__ uint64_t codes64(const uint32_t* words, uint32_t b) {
+    const uint32_t w = b >> 4;
+    const uint32_t sh = (b & 15u) * 2u;
     const uint32_t w0 = words[w], w1 = words[w + 1], w2 = words[w + 2];
     const uint32_t lo = __funnelshift_r(w0, w1, sh);
     const uint32_t hi = __funnelshift_r(w1, w2, sh);
@@ -85,9 +86,9 @@ __device__ __forceinline__ uint64_t codes64(const uint32_t* words, uint64_t b) {
 }
 
 // 64 bits of a bitmap starting at bit b (words of 32 bits); reads words b/32 .. b/32+2.
-__device__ __forceinline__ uint64_t bits64(const uint32_t* words, uint64_t b) {
-    const uint64_t w = b >> 5;
-    const uint32_t sh = (uint32_t)(b & 31);
+__device__ __forceinline__ uint64_t bits64(const uint32_t* words, uint32_t b) {
+    const uint32_t w = b >> 5;
+    const uint32_t sh = b & 31u;
     const uint32_t w0 = words[w], w1 = words[w + 1], w2 = words[w + 2];
     const uint32_t lo = __funnelshift_r(w0, w1, sh);
     const uint32_t hi = __funnelshift_r(w1, w2, sh);

@@ -374,12 +374,12 @@ __device__ __forceinline__ void nt_direct_tab(const TileSmem& sm, uint64_t v, ui
 }
 
 // Block id of the super-k-mer whose minimizer m-mer starts at relative base b.
-__device__ __forceinline__ uint32_t minimizer_block(const uint32_t* codes_s, uint64_t b, const DevGeom& g) {
+__device__ __forceinline__ uint32_t minimizer_block(const uint32_t* codes_s, uint32_t b, const DevGeom& g) {
     const uint64_t mm = codes64(codes_s, b) & len_mask(g.m);
     return (uint32_t)(xorshift64(canonical(mm, g.m)) & g.block_mask);
 }
 
-__device__ __forceinline__ uint32_t code_at(const uint32_t* words, uint64_t b) {
+__device__ __forceinline__ uint32_t code_at(const uint32_t* words, uint32_t b) {
     return (words[b >> 4] >> (2 * (b & 15))) & 3u;
 }
 
@@ -1136,9 +1136,10 @@ struct ApplyLayout {
 
 // s-mers (and windows) of one staged chunk of records; a record has at most 31 + 31
 constexpr uint32_t kSmerBudget = 2048;
-// 2-bit code words staged per record: its <= 62 bases from a 16-base boundary, plus the two
-// words codes64 reads past the last one
-constexpr uint32_t kRecBaseWords = 8;
+// 2-bit code words staged per record: its <= 61 bases (at most w = k - m + 1 windows of odd
+// k <= 31 bases) start at most 15 bases after a 16-base boundary, so they end in word 4.
+// codes64 may read up to two words further; those bits lie past the s-mer and are masked off.
+constexpr uint32_t kRecBaseWords = 5;
 
 __host__ __device__ inline uint32_t align16(uint32_t x) { return (x + 15u) & ~15u; }
 
@@ -1151,8 +1152,8 @@ __host__ __device__ inline ApplyLayout apply_layout(int mode, int bits, uint32_t
     l.spre = l.rv + align16(kApplyChunk * 8u);
     l.wpre = l.spre + align16((kApplyChunk + 1u) * 4u);
     l.bases = l.wpre + align16((kApplyChunk + 1u) * 4u);
-    l.rbases = l.bases + kApplyChunk * kRecBaseWords * 4u;
-    l.smap = l.rbases + kApplyChunk * kRecBaseWords * 4u + 16u;
+    l.rbases = l.bases + align16(kApplyChunk * kRecBaseWords * 4u);
+    l.smap = l.rbases + align16(kApplyChunk * kRecBaseWords * 4u + 16u);  // + the last record's over-read
     l.wmap = l.smap + align16(max_smers);
     l.touched = l.wmap + (mode == kModeInsert ? 0u : align16(max_windows));
     l.est = l.touched + align16(bucket_blocks);
