@@ -251,6 +251,27 @@ uint64_t items_bound(uint64_t n_buckets, uint64_t records) {
     return std::min<uint64_t>(n_buckets, records) + records / kItemRecords + 1;
 }
 
+// Probe slots kept between the insert and the query of the same records: one 64-bit word per
+// s-mer holds its n_hashes slot indices when they fit.  The capacity is the batch's bytes (an
+// upper bound of its windows) plus k - s extra s-mers per estimated super-k-mer; items past it
+// hash again in the query.
+bool probes_fit(const scb_ctx* ctx) { return ctx->g.h * ctx->cfg.block_slots_exponent <= 64; }
+
+uint64_t probe_capacity(const scb_ctx* ctx, uint64_t n_bytes) {
+    return n_bytes + records_estimate(ctx, n_bytes) * (ctx->g.k - ctx->g.s);
+}
+
+// Turns on probe reuse in the apply arguments: the insert writes (and first clears the count),
+// the query of the same prepared records reads.
+scb_status attach_probes(Lane& L, int mode, uint64_t cap, GroupArgs& ga, cudaStream_t st) {
+    if (mode == kModeInsert) SCB_CUDA(cudaMemsetAsync(L.rec_count.as<unsigned long long>() + 1, 0, 8, st));
+    ga.probes = L.probes.as<unsigned long long>();
+    ga.item_base = L.item_base.as<unsigned long long>();
+    ga.probe_count = L.rec_count.as<unsigned long long>() + 1;
+    ga.probe_cap = cap;
+    return SCB_OK;
+}
+
 GroupedSizes grouped_sizes(const scb_ctx* ctx, uint64_t n_bytes, uint64_t min_records) {
     GroupedSizes z;
     const uint64_t est = records_estimate(ctx, n_bytes);
@@ -277,7 +298,7 @@ scb_status grouped_buffers(Lane& L, const GroupedSizes& z, uint64_t sorted_recor
 // The cut kernel: one record per super-k-mer into slots [0, z.cap) and the bucket histogram.
 scb_status launch_cut(scb_ctx* ctx, Lane& L, TileArgs& a, const GroupedSizes& z, cudaStream_t st) {
     SCB_CUDA(cudaMemsetAsync(L.bhist.p, 0, (z.n_buckets + 1) * 8, st));
-    SCB_CUDA(cudaMemsetAsync(L.rec_count.p, 0, 8, st));
+    SCB_CUDA(cudaMemsetAsync(L.rec_count.p, 0, 16, st));  // record slots, probe slots
     a.rec_key = L.rec_key.as<uint32_t>();
     a.rec_val = L.rec_val.as<unsigned long long>();
     a.rec_count = L.rec_count.as<unsigned long long>();
@@ -398,6 +419,13 @@ scb_status grouped_prepare(scb_ctx* ctx, Lane& L, TileArgs& a, cudaStream_t st) 
     SCB_TRY(grouped_buffers(L, z, produced));
     if (produced) SCB_TRY(launch_bucketing(ctx, L, z, st));
     gs.ga = group_args(ctx, L, a, z);
+    gs.probes_written = false;
+    gs.probe_cap = 0;
+    if (L.want_probes && produced) {
+        gs.probe_cap = probe_capacity(ctx, a.n_bytes);
+        SCB_TRY(L.probes.ensure(gs.probe_cap * 8));
+        SCB_TRY(L.item_base.ensure(z.max_items * 8));
+    }
     SCB_TRY(mark(ctx, L, 6, st));
     if (ctx->timing) L.spans |= kSpanCut;
     gs.valid = true;
@@ -409,7 +437,12 @@ scb_status grouped_apply(scb_ctx* ctx, Lane& L, int mode, unsigned long long* cn
     GroupedState& gs = L.gs;
     if (!gs.valid) return fail_kind(SCB_ERR_INTERNAL_STATE, "no prepared super-k-mer records");
     if (gs.produced == 0) return SCB_OK;
-    return launch_group_apply(ctx, L, mode, gs.ga, cnt, gs.max_items, st);
+    GroupArgs ga = gs.ga;
+    if (gs.probe_cap && (mode == kModeInsert || gs.probes_written)) {
+        SCB_TRY(attach_probes(L, mode, gs.probe_cap, ga, st));
+        if (mode == kModeInsert) gs.probes_written = true;
+    }
+    return launch_group_apply(ctx, L, mode, ga, cnt, gs.max_items, st);
 }
 
 scb_status run_grouped(scb_ctx* ctx, Lane& L, int mode, TileArgs& a, cudaStream_t st) {
@@ -507,7 +540,7 @@ constexpr size_t kMaxGraphsPerLane = 8;
 uint64_t lane_signature(const scb_ctx* ctx, const Lane& L) {
     const void* ptrs[] = {L.codes.p, L.valid.p, L.seqstart.p, L.cnt.p, L.cnt2.p, L.tiles.p, L.params.p,
                           L.rec_key.p, L.rec_val.p, L.rec_sorted.p, L.bhist.p, L.bcursor.p, L.icount.p,
-                          L.items.p, L.gscan.p, L.rec_count.p, ctx->table, ctx->status};
+                          L.items.p, L.gscan.p, L.rec_count.p, L.probes.p, L.item_base.p, ctx->table, ctx->status};
     uint64_t h = 0x243F6A8885A308D3ull;
     for (const void* q : ptrs) h = (h ^ (uint64_t)(uintptr_t)q) * 0x100000001B3ull + 0x9E3779B97F4A7C15ull;
     return h;
@@ -561,8 +594,9 @@ scb_status record_batch(scb_ctx* ctx, Lane& L, const GraphKey& K, cudaStream_t s
         SCB_TRY(mark(ctx, L, 2, st));
         if (K.s_ins == SCB_STRATEGY_GROUPED) {
             SCB_TRY(cut_and_bucket());
-            SCB_TRY(launch_group_apply(ctx, L, kModeInsert, group_args(ctx, L, a, z), L.cnt.as<unsigned long long>(),
-                                       z.max_items, st));
+            GroupArgs ga = group_args(ctx, L, a, z);
+            if (K.probe_cap) SCB_TRY(attach_probes(L, kModeInsert, K.probe_cap, ga, st));
+            SCB_TRY(launch_group_apply(ctx, L, kModeInsert, ga, L.cnt.as<unsigned long long>(), z.max_items, st));
         } else {
             SCB_TRY(run_tiles(ctx, L, kModeInsert, a, st));
         }
@@ -579,7 +613,9 @@ scb_status record_batch(scb_ctx* ctx, Lane& L, const GraphKey& K, cudaStream_t s
         launch_seq_windows_dyn(bp, ctx->g.k, qc, sms, st);
         if (K.s_query == SCB_STRATEGY_GROUPED) {
             if (!cut) SCB_TRY(cut_and_bucket());  // else: reuse the insert's records
-            SCB_TRY(launch_group_apply(ctx, L, kModeReport, group_args(ctx, L, a, z), qc, z.max_items, st));
+            GroupArgs ga = group_args(ctx, L, a, z);
+            if (K.probe_cap) SCB_TRY(attach_probes(L, kModeReport, K.probe_cap, ga, st));
+            SCB_TRY(launch_group_apply(ctx, L, kModeReport, ga, qc, z.max_items, st));
         } else {
             SCB_TRY(run_tiles(ctx, L, kModeReport, a, st));
         }
@@ -650,6 +686,12 @@ scb_status graph_batch(scb_ctx* ctx, Lane& L, int kind, const uint8_t* d_ascii, 
         K.max_items = z.max_items;
         K.apply_threads = ctx->tuning.apply_threads;
         SCB_TRY(grouped_buffers(L, z, z.cap));
+        if (kind == kBatchBuildStream && K.s_ins == SCB_STRATEGY_GROUPED && K.s_query == SCB_STRATEGY_GROUPED &&
+            probes_fit(ctx)) {
+            K.probe_cap = probe_capacity(ctx, cls);
+            SCB_TRY(L.probes.ensure(K.probe_cap * 8));
+            SCB_TRY(L.item_base.ensure(z.max_items * 8));
+        }
     }
     K.sig = lane_signature(ctx, L);
     // graphs whose nodes point at buffers that have since been replaced are dropped
@@ -719,7 +761,13 @@ scb_status run_batch(scb_ctx* ctx, Lane& L, int kind, const uint8_t* d_ascii, co
     TileArgs a;
     SCB_TRY(prepare_batch(ctx, L, d_ascii, d_offsets, n, n_bytes, st, a));
     if (kind != kBatchReport) {
-        SCB_TRY(insert_device_batch(ctx, L, a, st));
+        // a grouped build + stream query keeps the insert's probe slots for the query
+        L.want_probes = kind == kBatchBuildStream && probes_fit(ctx) &&
+                        resolve(ctx, ctx->insert_strategy, n_bytes, true) == SCB_STRATEGY_GROUPED &&
+                        resolve(ctx, ctx->query_strategy, n_bytes, false) == SCB_STRATEGY_GROUPED;
+        const scb_status rs = insert_device_batch(ctx, L, a, st);
+        L.want_probes = false;
+        SCB_TRY(rs);
         SCB_TRY(read_counters(ctx, L, st, c_ins));
     }
     if (kind != kBatchInsert) {

@@ -92,6 +92,8 @@ constexpr uint64_t kMaxBatchBytes = (1ull << 31);
 // Prepared grouped batch of a lane: sorted records and work items for the lane's current codes.
 struct GroupedState {
     bool valid = false;
+    bool probes_written = false;  // the insert apply stored every s-mer's probe slots
+    uint64_t probe_cap = 0;
     uint32_t shift = 0;
     uint64_t n_buckets = 0, max_items = 0, produced = 0;
     GroupArgs ga{};
@@ -123,12 +125,12 @@ enum BatchKind : int { kBatchInsert = 1, kBatchReport = 2, kBatchBuildStream = 3
 // sizes, plus a signature of the lane buffers the graph's nodes point at.
 struct GraphKey {
     int kind = 0, s_ins = 0, s_query = 0;
-    uint64_t cap_bytes = 0, rec_cap = 0, max_items = 0, n_buckets = 0;
+    uint64_t cap_bytes = 0, rec_cap = 0, max_items = 0, n_buckets = 0, probe_cap = 0;
     uint32_t shift = 0, apply_threads = 0;
     uint64_t sig = 0;
     bool operator==(const GraphKey& o) const {
         return kind == o.kind && s_ins == o.s_ins && s_query == o.s_query &&
-               cap_bytes == o.cap_bytes && rec_cap == o.rec_cap &&
+               cap_bytes == o.cap_bytes && rec_cap == o.rec_cap && probe_cap == o.probe_cap &&
                max_items == o.max_items && n_buckets == o.n_buckets && shift == o.shift &&
                apply_threads == o.apply_threads && sig == o.sig;
     }
@@ -146,6 +148,9 @@ struct Lane {
     DevBuf ascii, offsets, codes, valid, seqstart, woff, scan, wblock, wend, cnt, cnt2, tiles, params;
     // grouped pipeline: records, bucket offsets / cursors, work items
     DevBuf rec_key, rec_val, rec_sorted, bhist, bcursor, icount, items, gscan, rec_count;
+    // probe slots kept from a grouped insert for the query of the same records (build + stream)
+    DevBuf probes, item_base;
+    bool want_probes = false;
     cudaStream_t stream = nullptr;
     GroupedState gs;
     cudaEvent_t ev[kLaneEvents] = {};

@@ -1161,8 +1161,10 @@ __host__ __device__ inline ApplyLayout apply_layout(int mode, int bits, uint32_t
     return l;
 }
 
-template <int MODE, int BITS>
-__global__ void __launch_bounds__(kApplyMaxThreads) k_apply(GroupArgs a, uint32_t bs_log2, uint32_t bucket_blocks) {
+// NH = 4: four hashes per s-mer (the default geometry), unrolled, probe slots kept as 16-bit
+// lanes; NH = 0: any n_hashes, slots kept as block_slots_exponent-bit lanes.
+template <int MODE, int BITS, int NH>
+__device__ __forceinline__ void apply_body(const GroupArgs& a, uint32_t bs_log2, uint32_t bucket_blocks) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     using T = CounterTraits<BITS>;
     using Cnt = typename CounterType<BITS>::type;
@@ -1183,6 +1185,9 @@ __global__ void __launch_bounds__(kApplyMaxThreads) k_apply(GroupArgs a, uint32_
     uint8_t* touched = smem_raw + lay.touched;
     Est* est = reinterpret_cast<Est*>(smem_raw + lay.est);
     __shared__ uint4 item;
+    __shared__ unsigned item_idx;
+    __shared__ uint32_t item_smers;
+    __shared__ unsigned long long item_probes;
     __shared__ uint32_t warp_tot[2 * (kApplyMaxThreads / 32)];
 
     const uint32_t tid = threadIdx.x;
@@ -1197,6 +1202,8 @@ __global__ void __launch_bounds__(kApplyMaxThreads) k_apply(GroupArgs a, uint32_
         if (tid == 0) {
             const unsigned idx = atomicAdd(a.work_counter, 1u);
             item = idx < n_items ? a.items[idx] : make_uint4(0xFFFFFFFFu, 0, 0, 0);
+            item_idx = idx;
+            item_smers = 0;
         }
         __syncthreads();
         const uint4 it = item;
@@ -1205,6 +1212,33 @@ __global__ void __launch_bounds__(kApplyMaxThreads) k_apply(GroupArgs a, uint32_
         const uint64_t first = it.y;
         const uint32_t count = it.z;
         const bool exclusive = it.w != 0;
+
+        // probe slots of the item: the insert reserves room for all its s-mers, the query finds
+        // where the insert put them
+        unsigned long long pbase = kNoProbes;
+        if (a.probes) {
+            if constexpr (MODE == kModeInsert) {
+                uint32_t n = 0;
+                for (uint32_t r = tid; r < count; r += blockDim.x) {
+                    n += (uint32_t)((a.recs[first + r] >> kRecWindowsShift) & 63u) + ks;
+                }
+                n = __reduce_add_sync(0xFFFFFFFFu, n);
+                if ((tid & 31) == 0 && n) atomicAdd(&item_smers, n);
+                __syncthreads();
+                if (tid == 0) {
+                    unsigned long long b = atomicAdd(a.probe_count, (unsigned long long)item_smers);
+                    if (b + item_smers > a.probe_cap) b = kNoProbes;
+                    a.item_base[item_idx] = b;
+                    item_probes = b;
+                }
+            } else {
+                if (tid == 0) item_probes = a.item_base[item_idx];
+            }
+            __syncthreads();
+            pbase = item_probes;
+        }
+        const bool have_probes = MODE != kModeInsert && pbase != kNoProbes;
+        uint64_t poff = 0;  // s-mers of the item's earlier chunks
 
         for (uint32_t x = tid; x < bucket_blocks; x += blockDim.x) touched[x] = 0;
         if constexpr (MODE == kModeInsert) {
@@ -1232,8 +1266,9 @@ __global__ void __launch_bounds__(kApplyMaxThreads) k_apply(GroupArgs a, uint32_
             // the leading records whose s-mers fit the chunk's budget (at least one)
             const uint32_t nuse = (uint32_t)__syncthreads_count(tid < nrec && spre[tid + 1] <= kSmerBudget);
             // stage the records' bases, kRecBaseWords consecutive threads per record (one sector
-            // read, conflict-free shared stores), and their reverse complements
-            for (uint32_t x = tid; x < nuse * kRecBaseWords; x += blockDim.x) {
+            // read, conflict-free shared stores), and their reverse complements (a query with the
+            // insert's probe slots needs no bases)
+            for (uint32_t x = tid; x < (have_probes ? 0u : nuse * kRecBaseWords); x += blockDim.x) {
                 const uint32_t r = x / kRecBaseWords, j = x % kRecBaseWords;
                 const uint32_t cw = __ldg(a.codes + ((uint32_t)rv[r] >> 4) + j);
                 bases[x] = cw;
@@ -1253,9 +1288,30 @@ __global__ void __launch_bounds__(kApplyMaxThreads) k_apply(GroupArgs a, uint32_
             for (uint32_t f = tid; f < S; f += blockDim.x) {
                 const uint32_t r = smap[f];
                 const unsigned long long v = rv[r];
+                const uint32_t lb = (uint32_t)(v >> kRecLocalShift);
+                if constexpr (MODE != kModeInsert) {
+                    if (have_probes) {  // the insert's slots of this s-mer
+                        const unsigned long long pk = __ldcs(a.probes + pbase + poff + f);
+                        const Cell* blk = cells + (lb << bs_log2);
+                        uint32_t e;
+                        if constexpr (NH == 4) {
+                            const uint32_t lo = (uint32_t)pk, hi = (uint32_t)(pk >> 32);
+                            const uint32_t c0 = blk[lo & 0xFFFFu], c1 = blk[lo >> 16];
+                            const uint32_t c2 = blk[hi & 0xFFFFu], c3 = blk[hi >> 16];
+                            e = min(min(c0, c1), min(c2, c3));
+                        } else {
+                            e = T::kMax;
+                            for (uint32_t h = 0; h < g.h; h++) {
+                                const uint32_t c = blk[(uint32_t)(pk >> (h * bs_log2)) & (uint32_t)g.bs_mask];
+                                e = c < e ? c : e;
+                            }
+                        }
+                        est[f] = (Est)e;
+                        continue;
+                    }
+                }
                 const uint32_t start = (uint32_t)v;
                 const uint32_t rel = (start & 15u) + (f - spre[r]);  // base offset in the staged words
-                const uint32_t lb = (uint32_t)(v >> kRecLocalShift);
                 // forward s-mer from the staged words; its reverse complement from the mirrored
                 // words: base t of it is the complement of forward base rel + s - 1 - t, which
                 // sits at position 16 * kRecBaseWords - rel - s + t of the mirrored stream (bits
@@ -1265,19 +1321,45 @@ __global__ void __launch_bounds__(kApplyMaxThreads) k_apply(GroupArgs a, uint32_
                 uint64_t hash = xorshift64(fw < rc ? fw : rc);
                 Cell* blk = cells + (lb << bs_log2);
                 if constexpr (MODE == kModeInsert) {
-                    for (uint32_t h = 1;; h++) {  // n_hashes >= 1; no mix after the last probe
-                        atomicAdd(blk + (hash & g.bs_mask), 1u);
-                        if (h >= g.h) break;
-                        hash = xorshift64(hash);
+                    unsigned long long pk = 0;
+                    if constexpr (NH == 4) {
+                        uint32_t sl[4];
+#pragma unroll
+                        for (int j = 0; j < 4; j++) {
+                            sl[j] = (uint32_t)(hash & g.bs_mask);
+                            if (j < 3) hash = xorshift64(hash);  // no mix after the last probe
+                        }
+#pragma unroll
+                        for (int j = 0; j < 4; j++) atomicAdd(blk + sl[j], 1u);
+                        pk = (unsigned long long)(sl[0] | (sl[1] << 16)) |
+                             ((unsigned long long)(sl[2] | (sl[3] << 16)) << 32);
+                    } else {
+                        for (uint32_t h = 1;; h++) {  // n_hashes >= 1; no mix after the last probe
+                            const uint32_t slot = (uint32_t)(hash & g.bs_mask);
+                            atomicAdd(blk + slot, 1u);
+                            pk |= (unsigned long long)slot << ((h - 1) * bs_log2);
+                            if (h >= g.h) break;
+                            hash = xorshift64(hash);
+                        }
                     }
                     touched[lb] = 1;
+                    if (pbase != kNoProbes) __stcs(a.probes + pbase + poff + f, pk);
                 } else {
                     uint32_t e = T::kMax;
-                    for (uint32_t h = 1;; h++) {
-                        const uint32_t c = blk[hash & g.bs_mask];
-                        e = c < e ? c : e;
-                        if (h >= g.h) break;
-                        hash = xorshift64(hash);
+                    if constexpr (NH == 4) {
+#pragma unroll
+                        for (int j = 0; j < 4; j++) {
+                            const uint32_t c = blk[hash & g.bs_mask];
+                            e = c < e ? c : e;
+                            if (j < 3) hash = xorshift64(hash);
+                        }
+                    } else {
+                        for (uint32_t h = 1;; h++) {
+                            const uint32_t c = blk[hash & g.bs_mask];
+                            e = c < e ? c : e;
+                            if (h >= g.h) break;
+                            hash = xorshift64(hash);
+                        }
                     }
                     est[f] = (Est)e;
                 }
@@ -1297,6 +1379,7 @@ __global__ void __launch_bounds__(kApplyMaxThreads) k_apply(GroupArgs a, uint32_
                 __syncthreads();
             }
             c0 += nrec_used;
+            poff += S;
         }
 
         if constexpr (MODE == kModeInsert) {
@@ -1337,6 +1420,21 @@ __global__ void __launch_bounds__(kApplyMaxThreads) k_apply(GroupArgs a, uint32_
     warp_add_u64(&a.cnt[kCntChecksum], c_sum);
 }
 
+template <int MODE, int BITS, int NH>
+__global__ void __launch_bounds__(kApplyMaxThreads) k_apply_insert(GroupArgs a, uint32_t bs_log2,
+                                                                    uint32_t bucket_blocks) {
+    apply_body<MODE, BITS, NH>(a, bs_log2, bucket_blocks);
+}
+
+// The query is held to 2048 threads per SM at every CTA width (at most 32 registers), which
+// measured faster than the compiler's own choice; the insert measured faster without it.
+template <int MODE, int BITS, int NH>
+__global__ void __launch_bounds__(kApplyMaxThreads, 2048 / kApplyMaxThreads) k_apply_query(GroupArgs a,
+                                                                                           uint32_t bs_log2,
+                                                                                           uint32_t bucket_blocks) {
+    apply_body<MODE, BITS, NH>(a, bs_log2, bucket_blocks);
+}
+
 static size_t apply_smem(int mode, int bits, uint32_t bucket_slots, uint32_t bucket_blocks) {
     return apply_layout(mode, bits, bucket_slots, bucket_blocks).total;
 }
@@ -1345,7 +1443,12 @@ template <int MODE, int BITS>
 static void launch_apply_t(const GroupArgs& a, int bs_log2, uint32_t bucket_blocks, int sm_count, uint64_t max_items,
                            cudaStream_t st) {
     const size_t smem = apply_smem(MODE, BITS, (1u << bs_log2) * bucket_blocks, bucket_blocks);
-    auto fn = k_apply<MODE, BITS>;
+    void (*fn)(GroupArgs, uint32_t, uint32_t);
+    if constexpr (MODE == kModeInsert) {
+        fn = a.g.h == 4 ? k_apply_insert<MODE, BITS, 4> : k_apply_insert<MODE, BITS, 0>;
+    } else {
+        fn = a.g.h == 4 ? k_apply_query<MODE, BITS, 4> : k_apply_query<MODE, BITS, 0>;
+    }
     cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const int threads = (a.apply_threads == 128 || a.apply_threads == 512) ? (int)a.apply_threads : 256;
     int per_sm = 1;

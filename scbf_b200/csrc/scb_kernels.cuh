@@ -65,7 +65,16 @@ struct GroupArgs {
     // the batch with room for every record
     const unsigned long long* rec_count;
     uint64_t rec_cap;
+    // probe slots of every s-mer (n_hashes slot indices of block_slots_exponent bits, packed),
+    // written by an insert and read back by a query of the same records, which then skips the
+    // hashing.  item_base[i] = first entry of work item i, kNoProbes when the array was full (that
+    // item's query hashes again).  probes = nullptr: hash in every pass.
+    unsigned long long* probes;
+    unsigned long long* item_base;
+    unsigned long long* probe_count;
+    uint64_t probe_cap;
 };
+constexpr unsigned long long kNoProbes = ~0ull;
 
 // Slots of the per-launch 64-bit counter array.
 enum CounterSlot : int {

@@ -164,3 +164,42 @@ def test_server_batches_replay_graphs(scb, oracle_mod):
         ab, valid = idx.estimate_batch(d, o)
         assert np.array_equal(res[1], valid)
         assert np.array_equal(np.where(valid == 1, res[0], 0), np.where(valid == 1, ab, 0))
+
+
+@pytest.mark.parametrize("graphs", [True, False])
+def test_build_and_stream_probe_slots_overflow(scb, oracle_mod, graphs):
+    """A grouped build + stream query keeps the insert's probe slots for the query; poly-A reads
+    (one super-k-mer per window, seven s-mers each) outgrow the slots' capacity, so later work
+    items hash again.  Counts, report and table stay exact either way."""
+    import torch
+
+    from scbf_b200 import _lib, api
+
+    L = _lib.load()
+    cfg = scb.SuperCountingBloomConfig(k=31, m=21, s=25, n_hashes=4, counter_bits=scb.CounterBits(16),
+                                       counter_slots_exponent=22, block_slots_exponent=9, threads=3, queue=17)
+    data, offsets = scb.pack_sequences([b"A" * 100_000 for _ in range(20)] + _reads(31, 2000, 100, 900))
+    o = oracle_mod.OracleFilter(oracle_mod.make_config(31, 21, 25, 4, 16, 22, 9, 3, 17))
+    okm, osm = o.insert_batch_arrays(data, offsets)
+    oq = o.query_report_arrays(data, offsets)
+    assert osm > 2 * len(data)  # more s-mers than the probe slots hold
+    d_data = torch.from_numpy(data.copy()).to("cuda")
+    d_off = torch.from_numpy(offsets.view(np.int64).copy()).to("cuda")
+    km, sm = C.c_uint64(), C.c_uint64()
+    rep = _lib.ScbReport()
+    ctx = api._create(cfg)
+    assert L.scb_set_strategy(ctx.h, _lib.STRATEGIES["grouped"], _lib.STRATEGIES["grouped"]) == 0
+    assert L.scb_set_graphs(ctx.h, 1 if graphs else 0) == 0
+    for _ in range(2):
+        assert L.scb_reset(ctx.h) == 0
+        assert L.scb_build_and_stream_query_device(ctx.h, d_data.data_ptr(), d_off.data_ptr(), len(offsets) - 1,
+                                                   int(offsets[-1]), None, C.byref(km), C.byref(sm),
+                                                   C.byref(rep)) == 0, _lib.last_error()
+        assert (km.value, sm.value) == (okm, osm)
+        assert (rep.records_processed, rep.total_windows, rep.valid_kmers, rep.positive_estimates,
+                rep.estimate_checksum) == (oq.records_processed, oq.total_windows, oq.valid_kmers,
+                                           oq.positive_estimates, oq.estimate_checksum)
+    raw = np.zeros(int(L.scb_table_bytes(ctx.h)), dtype=np.uint8)
+    assert L.scb_table_download(ctx.h, raw.ctypes.data, raw.size) == 0
+    assert np.array_equal(raw, o.table().view(np.uint8))
+    ctx.close()
