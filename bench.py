@@ -415,6 +415,9 @@ def run_ours(args, dist: Dist):
                 "frac": achieved / peak, "peak_kind": peak_kind,
                 "traffic": kprof.get("dram_bytes_per_launch"),
                 "traffic_source": prof.get("source") if kprof else None,
+                # what HBM actually carried: the measured DRAM bytes of a launch over its time
+                "traffic_frac": (kprof["dram_bytes_per_launch"] / (dom_ms / 1e3) / 1e9 / peak)
+                if kprof.get("dram_bytes_per_launch") and dom_ms > 0 else None,
                 "algorithmic_bytes": alg, "kernel_ms": dom_ms,
                 "algorithmic_model": "random 32-byte sectors: 32 B x distinct sectors per super-k-mer "
                                      "(x2 for insert) + 2-bit packed reads",
