@@ -252,10 +252,11 @@ uint64_t items_bound(uint64_t n_buckets, uint64_t records) {
 }
 
 // Probe slots kept between the insert and the query of the same records: one 64-bit word per
-// s-mer holds its n_hashes slot indices when they fit.  The capacity is the batch's bytes (an
+// s-mer holds the bucket-cell indices of its n_hashes probes when there are at most four.  The capacity is the batch's bytes (an
 // upper bound of its windows) plus k - s extra s-mers per estimated super-k-mer; items past it
 // hash again in the query.
-bool probes_fit(const scb_ctx* ctx) { return ctx->g.h * ctx->cfg.block_slots_exponent <= 64; }
+// (kept as four 16-bit lanes of bucket-cell indices; buckets hold at most 16384 counters)
+bool probes_fit(const scb_ctx* ctx) { return ctx->g.h <= 4; }
 
 uint64_t probe_capacity(const scb_ctx* ctx, uint64_t n_bytes) {
     return n_bytes + records_estimate(ctx, n_bytes) * (ctx->g.k - ctx->g.s);

@@ -1140,6 +1140,8 @@ constexpr uint32_t kSmerBudget = 2048;
 // k <= 31 bases) start at most 15 bases after a 16-base boundary, so they end in word 4.
 // codes64 may read up to two words further; those bits lie past the s-mer and are masked off.
 constexpr uint32_t kRecBaseWords = 5;
+// probe-slot loads a query thread keeps in flight
+constexpr uint32_t kProbeBatch = 4;
 
 __host__ __device__ inline uint32_t align16(uint32_t x) { return (x + 15u) & ~15u; }
 
@@ -1161,8 +1163,9 @@ __host__ __device__ inline ApplyLayout apply_layout(int mode, int bits, uint32_t
     return l;
 }
 
-// NH = 4: four hashes per s-mer (the default geometry), unrolled, probe slots kept as 16-bit
-// lanes; NH = 0: any n_hashes, slots kept as block_slots_exponent-bit lanes.
+// NH = 4: four hashes per s-mer (the default geometry), unrolled; NH = 0: any n_hashes.  Kept
+// probe slots are 16-bit lanes (n_hashes <= 4), each the counter's index within the bucket's
+// shared-memory cells, so the query needs neither the s-mer nor its record.
 template <int MODE, int BITS, int NH>
 __device__ __forceinline__ void apply_body(const GroupArgs& a, uint32_t bs_log2, uint32_t bucket_blocks) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1274,8 +1277,8 @@ __device__ __forceinline__ void apply_body(const GroupArgs& a, uint32_t bs_log2,
                 bases[x] = cw;
                 rbases[r * kRecBaseWords + (kRecBaseWords - 1 - j)] = revcomp16(cw);
             }
-            if (tid < nuse) {  // record index of its s-mers / windows
-                const uint32_t s0 = spre[tid], s1 = spre[tid + 1];
+            if (tid < nuse) {  // record index of its s-mers (not needed with kept slots) / windows
+                const uint32_t s0 = spre[tid], s1 = have_probes ? s0 : spre[tid + 1];
                 for (uint32_t f = s0; f < s1; f++) smap[f] = (uint8_t)tid;
                 if constexpr (MODE == kModeReport) {
                     const uint32_t w0i = wpre[tid], w1i = wpre[tid + 1];
@@ -1285,31 +1288,45 @@ __device__ __forceinline__ void apply_body(const GroupArgs& a, uint32_t bs_log2,
             __syncthreads();
             const uint32_t nrec_used = nuse;
             const uint32_t S = spre[nrec_used];
-            for (uint32_t f = tid; f < S; f += blockDim.x) {
+            if constexpr (MODE != kModeInsert) {
+                if (have_probes) {
+                    // the insert's slots of the chunk's s-mers: kProbeBatch loads in flight per
+                    // thread, then the counter minima from shared memory
+                    const unsigned long long* src = a.probes + pbase + poff;
+                    for (uint32_t f0 = tid; f0 < S; f0 += kProbeBatch * blockDim.x) {
+                        unsigned long long pk[kProbeBatch];
+#pragma unroll
+                        for (uint32_t j = 0; j < kProbeBatch; j++) {
+                            const uint32_t f = f0 + j * blockDim.x;
+                            pk[j] = f < S ? __ldcs(src + f) : 0ull;
+                        }
+#pragma unroll
+                        for (uint32_t j = 0; j < kProbeBatch; j++) {
+                            const uint32_t f = f0 + j * blockDim.x;
+                            if (f >= S) break;
+                            uint32_t e;
+                            if constexpr (NH == 4) {
+                                const uint32_t lo = (uint32_t)pk[j], hi = (uint32_t)(pk[j] >> 32);
+                                const uint32_t c0 = cells[lo & 0xFFFFu], c1 = cells[lo >> 16];
+                                const uint32_t c2 = cells[hi & 0xFFFFu], c3 = cells[hi >> 16];
+                                e = min(min(c0, c1), min(c2, c3));
+                            } else {
+                                e = T::kMax;
+                                for (uint32_t h = 0; h < g.h; h++) {
+                                    const uint32_t c = cells[(uint32_t)(pk[j] >> (16 * h)) & 0xFFFFu];
+                                    e = c < e ? c : e;
+                                }
+                            }
+                            est[f] = (Est)e;
+                        }
+                    }
+                }
+            }
+            // hash the s-mers (insert; query without stored slots)
+            for (uint32_t f = have_probes ? S : tid; f < S; f += blockDim.x) {
                 const uint32_t r = smap[f];
                 const unsigned long long v = rv[r];
                 const uint32_t lb = (uint32_t)(v >> kRecLocalShift);
-                if constexpr (MODE != kModeInsert) {
-                    if (have_probes) {  // the insert's slots of this s-mer
-                        const unsigned long long pk = __ldcs(a.probes + pbase + poff + f);
-                        const Cell* blk = cells + (lb << bs_log2);
-                        uint32_t e;
-                        if constexpr (NH == 4) {
-                            const uint32_t lo = (uint32_t)pk, hi = (uint32_t)(pk >> 32);
-                            const uint32_t c0 = blk[lo & 0xFFFFu], c1 = blk[lo >> 16];
-                            const uint32_t c2 = blk[hi & 0xFFFFu], c3 = blk[hi >> 16];
-                            e = min(min(c0, c1), min(c2, c3));
-                        } else {
-                            e = T::kMax;
-                            for (uint32_t h = 0; h < g.h; h++) {
-                                const uint32_t c = blk[(uint32_t)(pk >> (h * bs_log2)) & (uint32_t)g.bs_mask];
-                                e = c < e ? c : e;
-                            }
-                        }
-                        est[f] = (Est)e;
-                        continue;
-                    }
-                }
                 const uint32_t start = (uint32_t)v;
                 const uint32_t rel = (start & 15u) + (f - spre[r]);  // base offset in the staged words
                 // forward s-mer from the staged words; its reverse complement from the mirrored
@@ -1331,13 +1348,14 @@ __device__ __forceinline__ void apply_body(const GroupArgs& a, uint32_t bs_log2,
                         }
 #pragma unroll
                         for (int j = 0; j < 4; j++) atomicAdd(blk + sl[j], 1u);
-                        pk = (unsigned long long)(sl[0] | (sl[1] << 16)) |
-                             ((unsigned long long)(sl[2] | (sl[3] << 16)) << 32);
+                        const uint32_t cb = lb << bs_log2;  // the block's first cell in the bucket
+                        pk = (unsigned long long)((cb + sl[0]) | ((cb + sl[1]) << 16)) |
+                             ((unsigned long long)((cb + sl[2]) | ((cb + sl[3]) << 16)) << 32);
                     } else {
                         for (uint32_t h = 1;; h++) {  // n_hashes >= 1; no mix after the last probe
                             const uint32_t slot = (uint32_t)(hash & g.bs_mask);
                             atomicAdd(blk + slot, 1u);
-                            pk |= (unsigned long long)slot << ((h - 1) * bs_log2);
+                            pk |= (unsigned long long)((lb << bs_log2) + slot) << (((h - 1) & 3) * 16);
                             if (h >= g.h) break;
                             hash = xorshift64(hash);
                         }

@@ -65,7 +65,7 @@ struct GroupArgs {
     // the batch with room for every record
     const unsigned long long* rec_count;
     uint64_t rec_cap;
-    // probe slots of every s-mer (n_hashes slot indices of block_slots_exponent bits, packed),
+    // probe slots of every s-mer (n_hashes <= 4 bucket-cell indices, 16-bit lanes),
     // written by an insert and read back by a query of the same records, which then skips the
     // hashing.  item_base[i] = first entry of work item i, kNoProbes when the array was full (that
     // item's query hashes again).  probes = nullptr: hash in every pass.
