@@ -1616,8 +1616,22 @@ scb_status scb_autotune(scb_ctx* ctx, const uint8_t* seqs, const uint64_t* offse
 
     std::vector<Cand> cands = {{SCB_STRATEGY_PLAIN, 512, 256}, {SCB_STRATEGY_FUSED, 512, 256}};
     if (grouped_supported(ctx)) {
-        for (uint32_t b : {256u, 512u, 1024u, 2048u}) {
-            for (uint32_t t : {128u, 256u, 512u}) cands.push_back({SCB_STRATEGY_GROUPED, b, t});
+        // records-per-bucket targets that give the sample distinct bucket sizes; where the
+        // 4096-counter cap makes several alike, only the default (512) or the one nearest to it
+        // is measured, so a tie in noise never moves the setting
+        std::vector<std::pair<uint32_t, uint32_t>> shifts;  // (shift, target)
+        Tuning probe = ctx->tuning;
+        for (uint32_t b : {512u, 256u, 1024u, 2048u}) {
+            probe.bucket_records = b;
+            std::swap(probe, ctx->tuning);
+            const uint32_t sh = bucket_shift_for(ctx, records_estimate(ctx, total));
+            std::swap(probe, ctx->tuning);
+            bool seen = false;
+            for (auto& x : shifts) seen = seen || x.first == sh;
+            if (!seen) shifts.push_back({sh, b});
+        }
+        for (auto& x : shifts) {
+            for (uint32_t t : {256u, 512u}) cands.push_back({SCB_STRATEGY_GROUPED, x.second, t});
         }
     }
     Tuning best;

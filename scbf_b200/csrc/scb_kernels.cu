@@ -1135,7 +1135,7 @@ struct ApplyLayout {
 };
 
 // s-mers (and windows) of one staged chunk of records; a record has at most 31 + 31
-constexpr uint32_t kSmerBudget = 2048;
+constexpr uint32_t kSmerBudget = 4096;
 // 2-bit code words staged per record: its <= 61 bases (at most w = k - m + 1 windows of odd
 // k <= 31 bases) start at most 15 bases after a 16-base boundary, so they end in word 4.
 // codes64 may read up to two words further; those bits lie past the s-mer and are masked off.
@@ -1468,7 +1468,8 @@ static void launch_apply_t(const GroupArgs& a, int bs_log2, uint32_t bucket_bloc
         fn = a.g.h == 4 ? k_apply_query<MODE, BITS, 4> : k_apply_query<MODE, BITS, 0>;
     }
     cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    const int threads = (a.apply_threads == 128 || a.apply_threads == 512) ? (int)a.apply_threads : 256;
+    // one thread per staged record at least (256 or 512 threads)
+    const int threads = a.apply_threads == 512 ? 512 : (int)kApplyChunk;
     int per_sm = 1;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem) != cudaSuccess || per_sm < 1) {
         per_sm = 1;

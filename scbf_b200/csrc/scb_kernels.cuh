@@ -43,7 +43,7 @@ struct BatchParams {
 constexpr uint32_t kRecWindowsShift = 32;
 constexpr uint32_t kRecLocalShift = 38;
 constexpr uint32_t kItemRecords = 4096;    // records per work item (heavier buckets are split)
-constexpr uint32_t kApplyChunk = 128;      // records staged in shared memory at a time
+constexpr uint32_t kApplyChunk = 256;      // records staged in shared memory at a time (<= CTA width)
 constexpr uint32_t kMaxBucketSlots = 16384;  // counters of one bucket held in shared memory
 constexpr uint32_t kApplyMaxThreads = 512;
 
@@ -59,7 +59,7 @@ struct GroupArgs {
     const unsigned long long* n_items;
     unsigned int* work_counter;
     uint32_t bucket_shift;
-    uint32_t apply_threads;  // CTA width of the apply kernel: 128, 256 (default) or 512
+    uint32_t apply_threads;  // CTA width of the apply kernel: 256 (default) or 512
     // record slots the cut reserved and the capacity it had: when the count exceeds the capacity
     // (a graph replay whose records outgrew its class) the apply does nothing and the host redoes
     // the batch with room for every record
