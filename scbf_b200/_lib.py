@@ -135,6 +135,7 @@ def load(path: str | None = None):
         "scb_set_timing": (C.c_int, [ctxp, C.c_int]),
         "scb_get_timings": (C.c_int, [ctxp, C.POINTER(ScbTimings)]),
         "scb_set_graphs": (C.c_int, [ctxp, C.c_int]),
+        "scb_set_piece_bytes": (C.c_int, [ctxp, C.c_uint64]),
         "scb_graph_stats": (C.c_int, [ctxp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
         "scb_reset": (C.c_int, [ctxp]),
         "scb_query_report_device_noalloc": (C.c_int, [ctxp, vp, vp, C.c_uint64, C.c_uint64, vp,

@@ -84,9 +84,10 @@ void fill_geometry(scb_ctx* ctx) {
 
 scb_status check_offsets(const uint64_t* offsets, uint64_t n) {
     if (!offsets) return fail_kind(SCB_ERR_INTERNAL_STATE, "null offsets");
-    for (uint64_t i = 0; i < n; i++) {
-        if (offsets[i + 1] < offsets[i]) return fail_kind(SCB_ERR_INTERNAL_STATE, "offsets must be non-decreasing");
-    }
+    // branch-free, so the compiler vectorises it: millions of offsets in a few milliseconds
+    uint64_t bad = 0;
+    for (uint64_t i = 0; i < n; i++) bad |= (uint64_t)(offsets[i + 1] < offsets[i]);
+    if (bad) return fail_kind(SCB_ERR_INTERNAL_STATE, "offsets must be non-decreasing");
     return SCB_OK;
 }
 
@@ -105,6 +106,23 @@ struct Chunk {
     uint64_t byte0, byte1;  // bytes [byte0, byte1) of the caller's buffer
     uint64_t win0;          // first output window of the chunk
 };
+
+// Pieces of whole sequences of at most cap bytes (one longer sequence alone), found by binary
+// search over the (validated, non-decreasing) offsets; win0 is not filled.
+scb_status plan_pieces(const uint64_t* offsets, uint64_t n, uint64_t cap, std::vector<Chunk>& out) {
+    out.clear();
+    uint64_t s = 0;
+    while (s < n) {
+        const uint64_t* hi = std::upper_bound(offsets + s + 1, offsets + n + 1, offsets[s] + cap);
+        uint64_t e = (uint64_t)(hi - offsets) - 1;  // last index with offsets[e] <= offsets[s] + cap
+        if (e <= s) e = s + 1;
+        if (offsets[e] - offsets[s] > kMaxBatchBytes - 64)
+            return fail_kind(SCB_ERR_INTERNAL_STATE, "a single sequence longer than 2 GiB is not supported");
+        out.push_back(Chunk{s, e, offsets[s], offsets[e], 0});
+        s = e;
+    }
+    return SCB_OK;
+}
 
 scb_status plan_chunks(const uint64_t* offsets, uint64_t n, uint64_t k, uint64_t cap, std::vector<Chunk>& out) {
     out.clear();
@@ -526,12 +544,12 @@ scb_status read_counters(scb_ctx* ctx, Lane& L, cudaStream_t st, unsigned long l
 
 // ---------------------------------------------------------------------------------------
 // CUDA graphs per batch shape.  A batch of the persistent strategies (fused, grouped) replays
-// a graph captured for its shape class: the batch kind, the byte capacity (n rounded up to four
-// steps per octave, at least 64 KiB), the sequence capacity (a power of two, at least 256), the
-// strategies and the grouped pipeline's sizes for that capacity.  The batch's own sizes and
-// input pointers reach the kernels through a parameter block that the graph's first node copies
-// from pinned host memory, so one graph serves every batch of its class and a replay is a
-// single launch with no host round trip between the cut and the apply.  A replay whose
+// a graph captured for its shape class: the batch kind, the strategies, and for the grouped
+// pipeline the byte class (n rounded up to four steps per octave, at least 64 KiB) that sizes its
+// record slots, buckets and work items.  The batch's own sizes and input pointers reach the
+// kernels through a parameter block that a one-thread kernel writes just before the replay, and
+// the other kernels' grids do not depend on the batch, so one graph serves every batch of its
+// class and a replay has no host round trip between the cut and the apply.  A replay whose
 // super-k-mer records outgrow the class's slots applies nothing (the bucketing and apply
 // kernels check the count) and the batch is redone eagerly; the lane then captures with room
 // for that many records.  The plain strategy stays one launch per stage, eagerly.
@@ -551,16 +569,17 @@ uint64_t lane_signature(const scb_ctx* ctx, const Lane& L) {
 scb_status record_batch(scb_ctx* ctx, Lane& L, const GraphKey& K, cudaStream_t st) {
     const BatchParams* bp = L.params.as<BatchParams>();
     const int sms = ctx->sm_count;
-    SCB_CUDA(cudaMemcpyAsync(L.params.p, L.h_params, sizeof(BatchParams), cudaMemcpyHostToDevice, st));
     // capacity of the graph: its class for the grouped pipeline, else the lane's buffers
     const uint64_t cap = K.cap_bytes;
     const uint64_t groups = (cap + 31) / 32;
-    SCB_TRY(mark(ctx, L, 0, st));
-    launch_clear_dyn(bp, L.seqstart.as<uint32_t>(), nullptr, nullptr, sms, st);
-    launch_pack_dyn(bp, L.codes.as<uint32_t>(), L.valid.as<uint32_t>(), sms, st);
-    launch_seqstart_dyn(bp, L.seqstart.as<uint32_t>(), sms, st);
-    SCB_TRY(mark(ctx, L, 1, st));
-    SCB_CUDA(cudaMemsetAsync(L.cnt.p, 0, kCntSlots * 8, st));
+    if (K.kind != kBatchReportKept) {  // a kept batch's codes are still in the lane
+        SCB_TRY(mark(ctx, L, 0, st));
+        launch_clear_dyn(bp, L.seqstart.as<uint32_t>(), nullptr, nullptr, sms, st);
+        launch_pack_dyn(bp, L.codes.as<uint32_t>(), L.valid.as<uint32_t>(), sms, st);
+        launch_seqstart_dyn(bp, L.seqstart.as<uint32_t>(), sms, st);
+        SCB_TRY(mark(ctx, L, 1, st));
+        SCB_CUDA(cudaMemsetAsync(L.cnt.p, 0, kCntSlots * 8, st));
+    }
     TileArgs a;
     std::memset(&a, 0, sizeof(a));
     a.g = ctx->g;
@@ -581,7 +600,7 @@ scb_status record_batch(scb_ctx* ctx, Lane& L, const GraphKey& K, cudaStream_t s
     z.n_buckets = K.n_buckets;
     z.cap = K.rec_cap;
     z.max_items = K.max_items;
-    bool cut = false;
+    bool cut = K.kind == kBatchReportKept;  // the insert's records are kept
     auto cut_and_bucket = [&]() -> scb_status {
         SCB_TRY(mark(ctx, L, 4, st));
         SCB_TRY(launch_cut(ctx, L, a, z, st));
@@ -591,7 +610,7 @@ scb_status record_batch(scb_ctx* ctx, Lane& L, const GraphKey& K, cudaStream_t s
         cut = true;
         return SCB_OK;
     };
-    if (K.kind != kBatchReport) {
+    if (kind_inserts(K.kind)) {
         SCB_TRY(mark(ctx, L, 2, st));
         if (K.s_ins == SCB_STRATEGY_GROUPED) {
             SCB_TRY(cut_and_bucket());
@@ -603,9 +622,9 @@ scb_status record_batch(scb_ctx* ctx, Lane& L, const GraphKey& K, cudaStream_t s
         }
         SCB_TRY(mark(ctx, L, 3, st));
     }
-    if (K.kind != kBatchInsert) {
+    if (kind_queries(K.kind)) {
         unsigned long long* qc = L.cnt.as<unsigned long long>();
-        if (K.kind == kBatchBuildStream) {
+        if (K.kind == kBatchBuildStream || K.kind == kBatchReportKept) {
             qc = L.cnt2.as<unsigned long long>();
             SCB_CUDA(cudaMemsetAsync(qc, 0, kCntSlots * 8, st));
         }
@@ -657,44 +676,65 @@ scb_status capture_batch(scb_ctx* ctx, Lane& L, const GraphKey& K, GraphEntry& o
     return SCB_OK;
 }
 
-// Runs the batch as a graph replay when its strategies allow; done = false leaves it to the
-// eager path (graphs off, plain strategy, empty batch, capture failure, record overflow).
-scb_status graph_batch(scb_ctx* ctx, Lane& L, int kind, const uint8_t* d_ascii, const uint64_t* d_offsets, uint64_t n,
-                       uint64_t n_bytes, cudaStream_t st, unsigned long long* c_ins, unsigned long long* c_q,
-                       bool& done) {
-    done = false;
-    if (!ctx->graphs || n == 0 || n_bytes == 0) return SCB_OK;
+// A graph launched for a batch, finished (counters read, record count checked) later.
+struct GraphRun {
+    bool launched = false;
+    bool grouped = false;
+    int kind = 0;
     GraphKey K;
-    K.kind = kind;
-    if (kind != kBatchReport) K.s_ins = resolve(ctx, ctx->insert_strategy, n_bytes, true);
-    if (kind != kBatchInsert) K.s_query = resolve(ctx, ctx->query_strategy, n_bytes, false);
-    if (K.s_ins == SCB_STRATEGY_PLAIN || K.s_query == SCB_STRATEGY_PLAIN) return SCB_OK;
-    // the grouped pipeline's record slots, buckets and work items are sized for a byte class;
-    // the fused kernels take any batch that fits the lane's buffers (capacity: those buffers)
-    const uint64_t cls = std::max(n_bytes, std::min(class_bytes(n_bytes), kMaxBatchBytes - 64));
-    const bool grouped = K.s_ins == SCB_STRATEGY_GROUPED || K.s_query == SCB_STRATEGY_GROUPED;
-    // lane buffers grow in class steps, so growing batches recapture rarely
-    SCB_TRY(ensure_lane_work(ctx, L, cls));
-    K.cap_bytes = grouped ? cls : std::min<uint64_t>(L.seqstart.cap / 4 - kPadWords, (kMaxBatchBytes - 64) / 32) * 32;
-    SCB_TRY(L.params.ensure(sizeof(BatchParams)));
-    SCB_TRY(L.cnt2.ensure(kCntSlots * 8));
-    if (!L.h_params) SCB_CUDA(cudaMallocHost((void**)&L.h_params, sizeof(BatchParams)));
-    if (grouped) {
-        const GroupedSizes z = grouped_sizes(ctx, cls, L.rec_hint);
-        K.shift = z.shift;
-        K.n_buckets = z.n_buckets;
-        K.rec_cap = z.cap;
-        K.max_items = z.max_items;
-        K.apply_threads = ctx->tuning.apply_threads;
-        SCB_TRY(grouped_buffers(L, z, z.cap));
-        if (kind == kBatchBuildStream && K.s_ins == SCB_STRATEGY_GROUPED && K.s_query == SCB_STRATEGY_GROUPED &&
-            probes_fit(ctx)) {
-            K.probe_cap = probe_capacity(ctx, cls);
-            SCB_TRY(L.probes.ensure(K.probe_cap * 8));
-            SCB_TRY(L.item_base.ensure(z.max_items * 8));
+};
+
+// Keys, sizes, captures (first time) and launches the batch's graph on st without waiting for it;
+// run.launched = false leaves the batch to the eager path (graphs off, plain strategy, empty
+// batch, capture failure, kept records that came from the eager path).
+scb_status graph_launch(scb_ctx* ctx, Lane& L, int kind, const uint8_t* d_ascii, const uint64_t* d_offsets,
+                        uint64_t n, uint64_t n_bytes, cudaStream_t st, GraphRun& run) {
+    run = GraphRun();
+    run.kind = kind;
+    if (n == 0 || n_bytes == 0) return SCB_OK;
+    GraphKey K;
+    if (kind == kBatchReportKept) {  // runs whenever the kept records came from a graph
+        if (!L.kept_graph) return SCB_OK;
+        K = L.kept_key;  // the kept insert's sizes and buffers
+        K.kind = kBatchReportKept;
+        K.s_ins = 0;
+        K.s_query = SCB_STRATEGY_GROUPED;
+    } else {
+        if (!ctx->graphs) return SCB_OK;
+        K.kind = kind;
+        if (kind_inserts(kind)) K.s_ins = resolve(ctx, ctx->insert_strategy, n_bytes, true);
+        if (kind_queries(kind)) K.s_query = resolve(ctx, ctx->query_strategy, n_bytes, false);
+        if (K.s_ins == SCB_STRATEGY_PLAIN || K.s_query == SCB_STRATEGY_PLAIN) return SCB_OK;
+        if (kind == kBatchInsertKeep && (K.s_ins != SCB_STRATEGY_GROUPED || !probes_fit(ctx))) return SCB_OK;
+        // the grouped pipeline's record slots, buckets and work items are sized for a byte class;
+        // the fused kernels take any batch that fits the lane's buffers (capacity: those buffers)
+        const uint64_t cls = std::max(n_bytes, std::min(class_bytes(n_bytes), kMaxBatchBytes - 64));
+        const bool grouped = K.s_ins == SCB_STRATEGY_GROUPED || K.s_query == SCB_STRATEGY_GROUPED;
+        // lane buffers grow in class steps, so growing batches recapture rarely
+        SCB_TRY(ensure_lane_work(ctx, L, cls));
+        K.cap_bytes =
+            grouped ? cls : std::min<uint64_t>(L.seqstart.cap / 4 - kPadWords, (kMaxBatchBytes - 64) / 32) * 32;
+        SCB_TRY(L.params.ensure(sizeof(BatchParams)));
+        SCB_TRY(L.cnt2.ensure(kCntSlots * 8));
+        if (grouped) {
+            const GroupedSizes z = grouped_sizes(ctx, cls, L.rec_hint);
+            K.shift = z.shift;
+            K.n_buckets = z.n_buckets;
+            K.rec_cap = z.cap;
+            K.max_items = z.max_items;
+            K.apply_threads = ctx->tuning.apply_threads;
+            SCB_TRY(grouped_buffers(L, z, z.cap));
+            const bool keep = kind == kBatchInsertKeep ||
+                              (kind == kBatchBuildStream && K.s_ins == SCB_STRATEGY_GROUPED &&
+                               K.s_query == SCB_STRATEGY_GROUPED);
+            if (keep && probes_fit(ctx)) {
+                K.probe_cap = probe_capacity(ctx, cls);
+                SCB_TRY(L.probes.ensure(K.probe_cap * 8));
+                SCB_TRY(L.item_base.ensure(z.max_items * 8));
+            }
         }
+        K.sig = lane_signature(ctx, L);
     }
-    K.sig = lane_signature(ctx, L);
     // graphs whose nodes point at buffers that have since been replaced are dropped
     for (size_t i = 0; i < L.graphs.size();) {
         if (L.graphs[i].key.sig != K.sig) {
@@ -725,30 +765,60 @@ scb_status graph_batch(scb_ctx* ctx, Lane& L, int kind, const uint8_t* d_ascii, 
         L.graphs.push_back(fresh);
         ge = &L.graphs.back();
     }
-    *L.h_params = BatchParams{n_bytes, n, d_ascii, d_offsets};
+    launch_set_params(L.params.as<BatchParams>(), BatchParams{n_bytes, n, d_ascii, d_offsets}, st);
     SCB_CUDA(cudaGraphLaunch(ge->exec, st));
     note_launches(ge->launches);
     ge->last_use = ++L.graph_clock;
     L.replays++;
     L.gs.valid = false;
-    if (ctx->timing) {
-        L.spans = kSpanPack;
-        if (kind != kBatchReport) L.spans |= kSpanInsert | (K.s_ins == SCB_STRATEGY_GROUPED ? kSpanApplyInsert : 0u);
-        if (kind != kBatchInsert) L.spans |= kSpanQuery | (K.s_query == SCB_STRATEGY_GROUPED ? kSpanApplyQuery : 0u);
-        if (grouped) L.spans |= kSpanCut;
+    run.grouped = K.s_ins == SCB_STRATEGY_GROUPED || K.s_query == SCB_STRATEGY_GROUPED;
+    if (kind == kBatchInsertKeep) {
+        L.kept_graph = true;
+        L.kept_key = K;
     }
-    unsigned long long produced = 0;
-    if (grouped) SCB_CUDA(cudaMemcpyAsync(&produced, L.rec_count.p, 8, cudaMemcpyDeviceToHost, st));
-    if (kind == kBatchBuildStream) SCB_CUDA(cudaMemcpyAsync(c_q, L.cnt2.p, kCntSlots * 8, cudaMemcpyDeviceToHost, st));
-    SCB_TRY(read_counters(ctx, L, st, kind == kBatchReport ? c_q : c_ins));
-    if (grouped && produced > K.rec_cap) {
+    if (ctx->timing) {
+        L.spans = kind == kBatchReportKept ? 0u : (uint32_t)kSpanPack;
+        if (kind_inserts(kind)) L.spans |= kSpanInsert | (K.s_ins == SCB_STRATEGY_GROUPED ? kSpanApplyInsert : 0u);
+        if (kind_queries(kind)) L.spans |= kSpanQuery | (K.s_query == SCB_STRATEGY_GROUPED ? kSpanApplyQuery : 0u);
+        if (run.grouped && kind != kBatchReportKept) L.spans |= kSpanCut;
+    }
+    run.launched = true;
+    run.K = K;
+    return SCB_OK;
+}
+
+// Waits for a launched graph, reads its counters (c_ins: insert, c_q: query) and checks the
+// record count; done = false: the replay applied nothing and the batch goes to the eager path.
+scb_status graph_finish(scb_ctx* ctx, Lane& L, const GraphRun& run, cudaStream_t st, unsigned long long* c_ins,
+                        unsigned long long* c_q, bool& done) {
+    done = false;
+    if (!run.launched) return SCB_OK;
+    const int kind = run.kind;
+    const bool check = run.grouped && kind_inserts(kind);
+    unsigned long long produced = 0, scratch[kCntSlots];
+    if (check) SCB_CUDA(cudaMemcpyAsync(&produced, L.rec_count.p, 8, cudaMemcpyDeviceToHost, st));
+    if (kind == kBatchBuildStream || kind == kBatchReportKept) {
+        SCB_CUDA(cudaMemcpyAsync(c_q, L.cnt2.p, kCntSlots * 8, cudaMemcpyDeviceToHost, st));
+    }
+    unsigned long long* main = kind == kBatchReport ? c_q : kind == kBatchReportKept ? scratch : c_ins;
+    SCB_TRY(read_counters(ctx, L, st, main));
+    if (check && produced > run.K.rec_cap) {
         // nothing was applied: redo the batch eagerly and capture with room for these records
         L.rec_hint = produced + produced / 4;
         L.graph_fallbacks++;
+        if (kind == kBatchInsertKeep) L.kept_graph = false;
         return SCB_OK;
     }
     done = true;
     return SCB_OK;
+}
+
+scb_status graph_batch(scb_ctx* ctx, Lane& L, int kind, const uint8_t* d_ascii, const uint64_t* d_offsets, uint64_t n,
+                       uint64_t n_bytes, cudaStream_t st, unsigned long long* c_ins, unsigned long long* c_q,
+                       bool& done) {
+    GraphRun run;
+    SCB_TRY(graph_launch(ctx, L, kind, d_ascii, d_offsets, n, n_bytes, st, run));
+    return graph_finish(ctx, L, run, st, c_ins, c_q, done);
 }
 
 // One device batch of the given kind: a graph replay when possible, else the eager pipeline.
@@ -758,20 +828,34 @@ scb_status run_batch(scb_ctx* ctx, Lane& L, int kind, const uint8_t* d_ascii, co
     bool done = false;
     SCB_TRY(graph_batch(ctx, L, kind, d_ascii, d_offsets, n, n_bytes, st, c_ins, c_q, done));
     if (done) return SCB_OK;
+    if (kind == kBatchReportKept) {  // query the records an eager insert kept in this lane
+        if (!L.gs.valid) return fail_kind(SCB_ERR_INTERNAL_STATE, "no kept super-k-mer records for this batch");
+        TileArgs a;
+        std::memset(&a, 0, sizeof(a));
+        a.g = ctx->g;
+        a.n_bytes = n_bytes;
+        a.cnt = L.cnt.as<unsigned long long>();
+        SCB_CUDA(cudaMemsetAsync(L.cnt.p, 0, kCntSlots * 8, st));
+        launch_seq_windows(d_offsets, n, ctx->g.k, a.cnt, nullptr, st);
+        SCB_TRY(query_device_batch(ctx, L, kModeReport, a, st));
+        return read_counters(ctx, L, st, c_q);
+    }
     SCB_TRY(ensure_lane_work(ctx, L, n_bytes));
     TileArgs a;
     SCB_TRY(prepare_batch(ctx, L, d_ascii, d_offsets, n, n_bytes, st, a));
-    if (kind != kBatchReport) {
+    if (kind_inserts(kind)) {
         // a grouped build + stream query keeps the insert's probe slots for the query
-        L.want_probes = kind == kBatchBuildStream && probes_fit(ctx) &&
+        L.want_probes = (kind == kBatchBuildStream || kind == kBatchInsertKeep) && probes_fit(ctx) &&
                         resolve(ctx, ctx->insert_strategy, n_bytes, true) == SCB_STRATEGY_GROUPED &&
-                        resolve(ctx, ctx->query_strategy, n_bytes, false) == SCB_STRATEGY_GROUPED;
+                        (kind == kBatchInsertKeep ||
+                         resolve(ctx, ctx->query_strategy, n_bytes, false) == SCB_STRATEGY_GROUPED);
         const scb_status rs = insert_device_batch(ctx, L, a, st);
         L.want_probes = false;
         SCB_TRY(rs);
         SCB_TRY(read_counters(ctx, L, st, c_ins));
+        if (kind == kBatchInsertKeep) L.kept_graph = false;  // the lane's eager state holds the records
     }
-    if (kind != kBatchInsert) {
+    if (kind == kBatchBuildStream || kind == kBatchReport) {
         if (kind == kBatchBuildStream) SCB_CUDA(cudaMemsetAsync(L.cnt.p, 0, kCntSlots * 8, st));
         launch_seq_windows(d_offsets, n, ctx->g.k, a.cnt, nullptr, st);
         SCB_TRY(query_device_batch(ctx, L, kModeReport, a, st));
@@ -1132,6 +1216,123 @@ static scb_status build_stream_batch(scb_ctx* ctx, Lane& L, const uint8_t* d_seq
     return SCB_OK;
 }
 
+// Default sequence bytes per piece of a host build + stream query (whole sequences).
+constexpr uint64_t kPieceBytes = 768ull << 20;
+
+
+// Host build + stream query of a large batch in pieces, each in its own lane: piece p + 1 is
+// copied to the device on the copy stream while piece p's insert graph runs, every piece keeps
+// its super-k-mer records and probe slots, and after the last insert each piece's query runs on
+// what it kept.  done = false: the batch is not split (small, graphs off, or a strategy other
+// than grouped for some piece), and the caller runs it as one batch.
+static scb_status build_stream_pieces(scb_ctx* ctx, const uint8_t* seqs, const uint64_t* offsets, uint64_t n,
+                                      uint64_t* kmers, uint64_t* smers, scb_report* rep, bool& done) {
+    done = false;
+    const uint64_t total = n ? offsets[n] - offsets[0] : 0;
+    const uint64_t piece_bytes = ctx->piece_bytes ? ctx->piece_bytes : kPieceBytes;
+    if (!ctx->graphs || !probes_fit(ctx) || total < 2 * piece_bytes) return SCB_OK;
+    std::vector<Chunk> pieces;
+    SCB_TRY(plan_pieces(offsets, n, piece_bytes, pieces));
+    if (pieces.size() < 2) return SCB_OK;
+    for (const Chunk& c : pieces) {
+        const uint64_t b = c.byte1 - c.byte0;
+        if (resolve(ctx, ctx->insert_strategy, b, true) != SCB_STRATEGY_GROUPED ||
+            resolve(ctx, ctx->query_strategy, b, false) != SCB_STRATEGY_GROUPED) {
+            return SCB_OK;
+        }
+    }
+    const size_t P = pieces.size();
+    while (ctx->piece_lanes.size() < P) ctx->piece_lanes.push_back(std::make_unique<Lane>());
+    while (ctx->piece_events.size() < P) {
+        cudaEvent_t e;
+        SCB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        ctx->piece_events.push_back(e);
+    }
+    if (!ctx->copy_stream) SCB_CUDA(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+    Lane& main = ctx->lane;
+    SCB_TRY(ensure_lane_work(ctx, main, 0));  // its stream runs the pieces
+    cudaStream_t cs = main.stream, xs = ctx->copy_stream;
+    // pinned reads are copied asynchronously; pageable ones block the host per copy, which still
+    // overlaps the GPU's work on the pieces already launched
+    auto upload = [&](size_t p) -> scb_status {
+        const Chunk& c = pieces[p];
+        Lane& L = *ctx->piece_lanes[p];
+        const uint64_t ns = c.seq1 - c.seq0, nb = c.byte1 - c.byte0;
+        SCB_TRY(ensure_lane(ctx, L, nb, ns));
+        SCB_CUDA(cudaMemcpyAsync(L.ascii.p, seqs + c.byte0, nb, cudaMemcpyHostToDevice, xs));
+        SCB_CUDA(cudaMemcpyAsync(L.offsets.p, offsets + c.seq0, (ns + 1) * 8, cudaMemcpyHostToDevice, xs));
+        SCB_CUDA(cudaEventRecord(ctx->piece_events[p], xs));
+        return SCB_OK;
+    };
+    std::vector<GraphRun> runs(P);
+    SCB_TRY(upload(0));
+    for (size_t p = 0; p < P; p++) {
+        const Chunk& c = pieces[p];
+        Lane& L = *ctx->piece_lanes[p];
+        const uint64_t ns = c.seq1 - c.seq0, nb = c.byte1 - c.byte0;
+        SCB_CUDA(cudaStreamWaitEvent(cs, ctx->piece_events[p], 0));
+        if (c.byte0) {
+            k_rebase<<<(unsigned)((ns + 1 + 255) / 256), 256, 0, cs>>>(L.offsets.as<uint64_t>(), ns + 1, c.byte0);
+            note_launch();
+        }
+        SCB_TRY(graph_launch(ctx, L, kBatchInsertKeep, L.ascii.as<uint8_t>(), L.offsets.as<uint64_t>(), ns, nb, cs,
+                             runs[p]));
+        if (!runs[p].launched) {  // no graph: the eager insert (it waits for its own results)
+            unsigned long long c_ins[kCntSlots] = {};
+            SCB_TRY(run_batch(ctx, L, kBatchInsertKeep, L.ascii.as<uint8_t>(), L.offsets.as<uint64_t>(), ns, nb, cs,
+                              c_ins, nullptr));
+            ctx->inserted_kmers += c_ins[kCntWindows];
+            ctx->inserted_smers += c_ins[kCntSmers];
+            if (kmers) *kmers += c_ins[kCntWindows];
+            if (smers) *smers += c_ins[kCntSmers];
+        }
+        if (p + 1 < P) SCB_TRY(upload(p + 1));
+    }
+    for (size_t p = 0; p < P; p++) {
+        if (!runs[p].launched) continue;
+        const Chunk& c = pieces[p];
+        Lane& L = *ctx->piece_lanes[p];
+        const uint64_t ns = c.seq1 - c.seq0, nb = c.byte1 - c.byte0;
+        unsigned long long c_ins[kCntSlots] = {};
+        bool ok = false;
+        SCB_TRY(graph_finish(ctx, L, runs[p], cs, c_ins, nullptr, ok));
+        if (!ok) {  // records outgrew the class: nothing was applied, insert it eagerly
+            std::memset(c_ins, 0, sizeof(c_ins));
+            SCB_TRY(run_batch(ctx, L, kBatchInsertKeep, L.ascii.as<uint8_t>(), L.offsets.as<uint64_t>(), ns, nb, cs,
+                              c_ins, nullptr));
+        }
+        ctx->inserted_kmers += c_ins[kCntWindows];
+        ctx->inserted_smers += c_ins[kCntSmers];
+        if (kmers) *kmers += c_ins[kCntWindows];
+        if (smers) *smers += c_ins[kCntSmers];
+    }
+    ctx->frozen = true;
+    for (size_t p = 0; p < P; p++) {
+        const Chunk& c = pieces[p];
+        Lane& L = *ctx->piece_lanes[p];
+        SCB_TRY(graph_launch(ctx, L, kBatchReportKept, L.ascii.as<uint8_t>(), L.offsets.as<uint64_t>(),
+                             c.seq1 - c.seq0, c.byte1 - c.byte0, cs, runs[p]));
+    }
+    for (size_t p = 0; p < P; p++) {
+        const Chunk& c = pieces[p];
+        Lane& L = *ctx->piece_lanes[p];
+        unsigned long long q[kCntSlots] = {};
+        bool ok = false;
+        SCB_TRY(graph_finish(ctx, L, runs[p], cs, nullptr, q, ok));
+        if (!ok) {
+            SCB_TRY(run_batch(ctx, L, kBatchReportKept, L.ascii.as<uint8_t>(), L.offsets.as<uint64_t>(),
+                              c.seq1 - c.seq0, c.byte1 - c.byte0, cs, nullptr, q));
+        }
+        rep->records_processed += q[kCntRecords];
+        rep->total_windows += q[kCntTotalWindows];
+        rep->valid_kmers += q[kCntValid];
+        rep->positive_estimates += q[kCntPositive];
+        rep->estimate_checksum += q[kCntChecksum];
+    }
+    done = true;
+    return SCB_OK;
+}
+
 scb_status scb_build_and_stream_query(scb_ctx* ctx, const uint8_t* seqs, const uint64_t* offsets, uint64_t n,
                                       uint64_t* kmers, uint64_t* smers, scb_report* rep) {
     if (!ctx || !rep) return fail_kind(SCB_ERR_INTERNAL_STATE, "null argument");
@@ -1140,6 +1341,12 @@ scb_status scb_build_and_stream_query(scb_ctx* ctx, const uint8_t* seqs, const u
         if (ctx->frozen) return fail_kind(SCB_ERR_INTERNAL_STATE, "the index is frozen; inserts need a builder");
         SCB_TRY(check_offsets(offsets, n));
         const uint64_t total = n ? offsets[n] - offsets[0] : 0;
+        std::memset(rep, 0, sizeof(*rep));
+        if (kmers) *kmers = 0;
+        if (smers) *smers = 0;
+        bool done = false;
+        SCB_TRY(build_stream_pieces(ctx, seqs, offsets, n, kmers, smers, rep, done));
+        if (done) return SCB_OK;
         if (total <= kMaxBatchBytes - 64) {
             // one resident batch: copy once, insert, freeze, query the same staged codes (and,
             // with the grouped strategy, the same super-k-mer records)
@@ -1337,6 +1544,13 @@ scb_status scb_set_graphs(scb_ctx* ctx, int enable) {
     if (!ctx) return fail_kind(SCB_ERR_INTERNAL_STATE, "null context");
     CtxLock lk(ctx);
     ctx->graphs = enable != 0;
+    return SCB_OK;
+}
+
+scb_status scb_set_piece_bytes(scb_ctx* ctx, uint64_t piece_bytes) {
+    if (!ctx) return fail_kind(SCB_ERR_INTERNAL_STATE, "null context");
+    CtxLock lk(ctx);
+    ctx->piece_bytes = piece_bytes;
     return SCB_OK;
 }
 

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -119,7 +120,18 @@ inline uint64_t class_bytes(uint64_t n) {
 }
 
 // Kinds of batch a lane runs, eagerly or as a replay of a captured graph.
-enum BatchKind : int { kBatchInsert = 1, kBatchReport = 2, kBatchBuildStream = 3 };
+// kBatchInsertKeep inserts and keeps the batch's records and probe slots in its lane, and
+// kBatchReportKept queries them after the table is complete (a build + stream query split into
+// pieces, each on its own lane).
+enum BatchKind : int {
+    kBatchInsert = 1,
+    kBatchReport = 2,
+    kBatchBuildStream = 3,
+    kBatchInsertKeep = 4,
+    kBatchReportKept = 5
+};
+inline bool kind_inserts(int kind) { return kind == kBatchInsert || kind == kBatchBuildStream || kind == kBatchInsertKeep; }
+inline bool kind_queries(int kind) { return kind == kBatchReport || kind == kBatchBuildStream || kind == kBatchReportKept; }
 
 // Shape class of a graph: batch kind, strategies, byte capacity and the grouped pipeline's
 // sizes, plus a signature of the lane buffers the graph's nodes point at.
@@ -155,18 +167,19 @@ struct Lane {
     GroupedState gs;
     cudaEvent_t ev[kLaneEvents] = {};
     uint32_t spans = 0;
-    // captured graphs of this lane by shape class, the pinned parameter block their first node
-    // copies to the device, and the record capacity learned from overflowing replays
+    // captured graphs of this lane by shape class and the record capacity learned from
+    // overflowing replays
     std::vector<GraphEntry> graphs;
-    BatchParams* h_params = nullptr;
     uint64_t rec_hint = 0;
     bool recording = false;  // a stream capture of this lane is in progress
+    // records and probe slots kept by a kBatchInsertKeep replay of this key for kBatchReportKept
+    bool kept_graph = false;
+    GraphKey kept_key;
     uint64_t graph_clock = 0, captures = 0, replays = 0, graph_fallbacks = 0;
     ~Lane() {
         for (auto& g : graphs) {
             if (g.exec) cudaGraphExecDestroy(g.exec);
         }
-        if (h_params) cudaFreeHost(h_params);
         for (auto& e : ev) {
             if (e) cudaEventDestroy(e);
         }
@@ -204,11 +217,19 @@ struct scb_ctx {
     scb_strategy insert_strategy = SCB_STRATEGY_AUTO, query_strategy = SCB_STRATEGY_AUTO;
     scb::Tuning tuning;
     scb::Lane lane;
+    // a host build + stream query in pieces: one lane per piece, uploads on their own stream
+    std::vector<std::unique_ptr<scb::Lane>> piece_lanes;
+    cudaStream_t copy_stream = nullptr;
+    std::vector<cudaEvent_t> piece_events;
+    uint64_t piece_bytes = 0;  // 0: the default
     bool timing = false;
     bool graphs = true;  // replay batches through graphs captured per shape class
     scb_timings times{};
     std::mutex mu;
     ~scb_ctx() {
+        for (auto e : piece_events) cudaEventDestroy(e);
+        if (copy_stream) cudaStreamDestroy(copy_stream);
+        piece_lanes.clear();
         if (table) cudaFree(table);
         if (status) cudaFree(status);
     }

@@ -197,6 +197,15 @@ __global__ void k_seq_windows_dyn(const BatchParams* __restrict__ bp, uint32_t k
     warp_add_u64(&cnt[kCntRecords], recs);
 }
 
+// Writes a batch's parameter block from kernel arguments (ahead of a graph replay), so the
+// replay never waits on a copy engine that a large upload keeps busy.
+__global__ void k_set_params(BatchParams* bp, BatchParams v) { *bp = v; }
+
+void launch_set_params(BatchParams* bp, const BatchParams& v, cudaStream_t st) {
+    k_set_params<<<1, 1, 0, st>>>(bp, v);
+    note_launch();
+}
+
 void launch_pack_dyn(const BatchParams* bp, uint32_t* codes, uint32_t* valid, int sm_count, cudaStream_t st) {
     k_pack_dyn<<<(unsigned)(sm_count * 8), 256, 0, st>>>(bp, codes, valid);
     note_launch();

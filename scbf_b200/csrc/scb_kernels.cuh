@@ -143,6 +143,7 @@ void launch_pack(const uint8_t* ascii, uint64_t n_bytes, uint32_t* codes, uint32
 // device memory; grids are fixed (grid-stride loops over the batch), so one capture serves any
 // batch that fits the buffers.  The out / out_valid buffers of launch_clear_dyn need 16-byte
 // alignment and room for n_bytes rounded up to 16.
+void launch_set_params(BatchParams* bp, const BatchParams& v, cudaStream_t st);
 void launch_pack_dyn(const BatchParams* bp, uint32_t* codes, uint32_t* valid, int sm_count, cudaStream_t st);
 void launch_clear_dyn(const BatchParams* bp, uint32_t* seqstart, unsigned long long* out, uint8_t* out_valid,
                       int sm_count, cudaStream_t st);

@@ -8,7 +8,7 @@
 // launches it on the slot's stream: H2D copy, 2-bit packing, the fused per-window abundance
 // kernel, D2H copy.  The device work of a batch (clears, packing, sequence starts, abundance
 // kernel) is one replay of a CUDA graph captured once per slot: the batch's sizes reach the
-// kernels through a parameter block that the graph copies from the slot's pinned memory, and the
+// kernels through a parameter block that a one-thread kernel writes before the replay, and the
 // kernels' grids do not depend on the batch, so the same graph serves every batch shape.
 // Batches of different slots overlap on the GPU; requests that arrive while
 // others run are admitted as soon as a slot frees.  A host callback at the end of each batch
@@ -63,7 +63,6 @@ struct Piece {
 struct Slot {
     cudaStream_t stream = nullptr;
     DevBuf ascii, offsets, woff, codes, valid, seqstart, out, outv, cnt, tiles, params;
-    BatchParams* h_params = nullptr;
     cudaGraphExec_t graph = nullptr;  // the slot's batch, captured at its first batch
     uint64_t graph_launches = 0;
     uint8_t* h_ascii = nullptr;
@@ -77,7 +76,6 @@ struct Slot {
     std::atomic<bool> complete{false};
     ~Slot() {
         if (graph) cudaGraphExecDestroy(graph);
-        if (h_params) cudaFreeHost(h_params);
         if (h_ascii) cudaFreeHost(h_ascii);
         if (h_offsets) cudaFreeHost(h_offsets);
         if (h_woff) cudaFreeHost(h_woff);
@@ -164,7 +162,6 @@ static TileArgs tile_args(const scb_server& srv, const Slot& s, uint64_t bytes, 
 scb_status scb_server::record(Slot& s, cudaStream_t st) {
     const BatchParams* bp = s.params.as<BatchParams>();
     const int sms = ctx->sm_count;
-    SCB_CUDA(cudaMemcpyAsync(s.params.p, s.h_params, sizeof(BatchParams), cudaMemcpyHostToDevice, st));
     SCB_CUDA(cudaMemsetAsync(s.cnt.p, 0, kCntSlots * 8, st));
     SCB_CUDA(cudaMemsetAsync(s.tiles.p, 0, 64, st));
     launch_clear_dyn(bp, s.seqstart.as<uint32_t>(), s.out.as<unsigned long long>(), s.outv.as<uint8_t>(), sms, st);
@@ -226,7 +223,8 @@ scb_status scb_server::launch(Slot& s) {
     if (seqs) SCB_CUDA(cudaMemcpyAsync(s.woff.p, s.h_woff, seqs * 8, cudaMemcpyHostToDevice, st));
     if (bytes && use_graphs) {
         if (!s.graph) SCB_TRY(capture(s));
-        *s.h_params = BatchParams{bytes, seqs, s.ascii.as<uint8_t>(), s.offsets.as<uint64_t>()};
+        launch_set_params(s.params.as<BatchParams>(),
+                          BatchParams{bytes, seqs, s.ascii.as<uint8_t>(), s.offsets.as<uint64_t>()}, st);
         SCB_CUDA(cudaGraphLaunch(s.graph, st));
         note_launches(s.graph_launches);
         replays++;
@@ -385,7 +383,6 @@ scb_status scb_server_create(scb_ctx* ctx, const scb_server_config* cfg_in, scb_
         SCB_TRY(s->cnt.ensure(kCntSlots * 8));
         SCB_TRY(s->tiles.ensure(64));
         SCB_TRY(s->params.ensure(sizeof(BatchParams)));
-        SCB_CUDA(cudaMallocHost((void**)&s->h_params, sizeof(BatchParams)));
         SCB_CUDA(cudaMallocHost((void**)&s->h_ascii, B + 64));
         SCB_CUDA(cudaMallocHost((void**)&s->h_offsets, (R + 1) * 8));
         SCB_CUDA(cudaMallocHost((void**)&s->h_woff, (R + 1) * 8));

@@ -203,3 +203,49 @@ def test_build_and_stream_probe_slots_overflow(scb, oracle_mod, graphs):
     assert L.scb_table_download(ctx.h, raw.ctypes.data, raw.size) == 0
     assert np.array_equal(raw, o.table().view(np.uint8))
     ctx.close()
+
+
+@pytest.mark.parametrize("pinned", [False, True])
+def test_host_build_and_stream_in_pieces_matches_oracle(scb, oracle_mod, pinned):
+    """The host build + stream query split into pieces (copy of piece p + 1 overlapping the insert
+    of piece p, each piece queried on its kept records after the last insert) gives exactly the
+    oracle's counts, report and table, from pageable or pinned host memory."""
+    import torch
+
+    from scbf_b200 import _lib, api
+
+    L = _lib.load()
+    cfg = scb.SuperCountingBloomConfig(k=31, m=21, s=25, n_hashes=4, counter_bits=scb.CounterBits(16),
+                                       counter_slots_exponent=22, block_slots_exponent=9, threads=3, queue=17)
+    data, offsets = scb.pack_sequences(_reads(51, 9000, 100, 1200))
+    o = oracle_mod.OracleFilter(oracle_mod.make_config(31, 21, 25, 4, 16, 22, 9, 3, 17))
+    okm, osm = o.insert_batch_arrays(data, offsets)
+    oq = o.query_report_arrays(data, offsets)
+    if pinned:
+        h_data = torch.from_numpy(data.copy()).pin_memory()
+        h_off = torch.from_numpy(offsets.view(np.int64).copy()).pin_memory()
+        dp, op = h_data.data_ptr(), h_off.data_ptr()
+    else:
+        h_data, h_off = data, offsets
+        dp, op = data.ctypes.data, offsets.ctypes.data
+    ctx = api._create(cfg)
+    assert L.scb_set_strategy(ctx.h, _lib.STRATEGIES["grouped"], _lib.STRATEGIES["grouped"]) == 0
+    assert L.scb_set_piece_bytes(ctx.h, 1 << 20) == 0  # about six pieces
+    km, sm = C.c_uint64(), C.c_uint64()
+    rep = _lib.ScbReport()
+    for _ in range(2):
+        assert L.scb_reset(ctx.h) == 0
+        assert L.scb_build_and_stream_query(ctx.h, dp, op, len(offsets) - 1, C.byref(km), C.byref(sm),
+                                            C.byref(rep)) == 0, _lib.last_error()
+        assert (km.value, sm.value) == (okm, osm)
+        assert (rep.records_processed, rep.total_windows, rep.valid_kmers, rep.positive_estimates,
+                rep.estimate_checksum) == (oq.records_processed, oq.total_windows, oq.valid_kmers,
+                                           oq.positive_estimates, oq.estimate_checksum)
+        cnt_k, cnt_s = C.c_uint64(), C.c_uint64()
+        assert L.scb_get_counts(ctx.h, C.byref(cnt_k), C.byref(cnt_s)) == 0
+        assert (cnt_k.value, cnt_s.value) == (okm, osm)
+    raw = np.zeros(int(L.scb_table_bytes(ctx.h)), dtype=np.uint8)
+    assert L.scb_table_download(ctx.h, raw.ctypes.data, raw.size) == 0
+    assert np.array_equal(raw, o.table().view(np.uint8))
+    del h_data, h_off
+    ctx.close()
