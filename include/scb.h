@@ -226,7 +226,7 @@ scb_status scb_graph_stats(const scb_ctx* ctx, uint64_t* captures, uint64_t* rep
 
 /* Host scb_build_and_stream_query in pieces (no counterpart in the reference; the reference's
  * parser thread feeds its workers the same way, src/api.rs:621-674).  A batch of at least two
- * pieces is split into pieces of whole sequences of about piece_bytes (0: 384 MiB); piece p + 1
+ * pieces is split into pieces of whole sequences of about piece_bytes (0: 768 MiB); piece p + 1
  * is copied to the device while piece p is inserted, every piece keeps its super-k-mer records
  * for its query after the last insert, so the copy overlaps the work.  Applies with graphs on and
  * the grouped strategy; results are identical to one batch. */
