@@ -129,6 +129,10 @@ scb_status scb_query_batch_device(scb_ctx* ctx, const uint8_t* d_seqs, const uin
                                   uint8_t* d_valid);
 /* Number of windows scb_query_batch writes for these offsets. */
 uint64_t scb_count_windows(const scb_ctx* ctx, const uint64_t* offsets, uint64_t n_seqs);
+/* AddReport::records_indexed of add_fasta (src/api.rs:640-642): records with at least one run of
+ * k A/C/G/T bases (either case), i.e. records that insert at least one k-mer.  Host-side scan that
+ * stops at each record's first such run. */
+uint64_t scb_records_indexed(const scb_ctx* ctx, const uint8_t* seqs, const uint64_t* offsets, uint64_t n_seqs);
 
 /* SuperCountingBloomIndex::query_fasta's reduction (src/api.rs:273-327): records, windows,
  * valid k-mers, positive estimates and the wrapping checksum, without per-window output. */

@@ -116,6 +116,7 @@ def load(path: str | None = None):
         "scb_query_batch": (C.c_int, [ctxp, vp, vp, C.c_uint64, vp, vp]),
         "scb_query_batch_device": (C.c_int, [ctxp, vp, vp, C.c_uint64, C.c_uint64, vp, vp, vp]),
         "scb_count_windows": (C.c_uint64, [ctxp, vp, C.c_uint64]),
+        "scb_records_indexed": (C.c_uint64, [ctxp, vp, vp, C.c_uint64]),
         "scb_query_report": (C.c_int, [ctxp, vp, vp, C.c_uint64, C.POINTER(ScbReport)]),
         "scb_query_report_device": (C.c_int, [ctxp, vp, vp, C.c_uint64, C.c_uint64, vp, C.POINTER(ScbReport)]),
         "scb_build_and_stream_query": (C.c_int, [ctxp, vp, vp, C.c_uint64, u64p, u64p, C.POINTER(ScbReport)]),

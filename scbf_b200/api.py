@@ -392,18 +392,7 @@ class SuperCountingBloomBuilder:
     def _records_indexed(self, data, offsets) -> int:
         """Records that inserted at least one k-mer (src/api.rs:640-642)."""
         data, offsets = _as_batch(data, offsets)
-        k = int(self._cfg.k)
-        ok = _is_acgt_mask(data[: int(offsets[-1])]) if len(offsets) > 1 else np.zeros(0, bool)
-        n = 0
-        for i in range(len(offsets) - 1):
-            a, b = int(offsets[i]), int(offsets[i + 1])
-            if b - a < k:
-                continue
-            seg = ok[a:b].astype(np.int8)
-            d = np.diff(np.concatenate(([0], seg, [0])))
-            if ((np.flatnonzero(d == -1) - np.flatnonzero(d == 1)) >= k).any():
-                n += 1
-        return n
+        return int(_lib.load().scb_records_indexed(self._ctx.h, _ptr(data), _ptr(offsets), len(offsets) - 1))
 
     def add_fasta(self, path) -> AddReport:
         """src/api.rs:140-158, 621-666."""

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -1045,6 +1046,28 @@ scb_status scb_get_strategy(const scb_ctx* ctx, scb_strategy* ins, scb_strategy*
     if (ins) *ins = resolve(ctx->insert_strategy);
     if (q) *q = resolve(ctx->query_strategy);
     return SCB_OK;
+}
+
+uint64_t scb_records_indexed(const scb_ctx* ctx, const uint8_t* seqs, const uint64_t* offsets, uint64_t n) {
+    if (!ctx || !seqs || !offsets) return 0;
+    static const auto acgt = [] {
+        std::array<uint8_t, 256> t{};
+        for (const char c : {'A', 'C', 'G', 'T', 'a', 'c', 'g', 't'}) t[(uint8_t)c] = 1;
+        return t;
+    }();
+    const uint64_t k = ctx->cfg.k;
+    uint64_t indexed = 0;
+    for (uint64_t j = 0; j < n; j++) {
+        uint64_t run = 0;
+        for (uint64_t p = offsets[j]; p < offsets[j + 1]; p++) {
+            run = acgt[seqs[p]] ? run + 1 : 0;
+            if (run >= k) {
+                indexed++;
+                break;
+            }
+        }
+    }
+    return indexed;
 }
 
 uint64_t scb_count_windows(const scb_ctx* ctx, const uint64_t* offsets, uint64_t n) {

@@ -346,3 +346,24 @@ def test_build_and_stream_query_device_matches_oracle(scb, oracle_mod, strategy)
         out = np.zeros(int(L.scb_table_bytes(b._ctx.h)), dtype=np.uint8)
         assert L.scb_table_download(b._ctx.h, out.ctypes.data, out.size) == 0
         assert np.array_equal(out.view(np.uint16), o.table())
+
+
+def test_records_indexed_matches_run_definition(scb):
+    """AddReport::records_indexed (src/api.rs:640-642): records holding a run of k A/C/G/T bases."""
+    seqs = _random_batch(77, 400, 1, 120, n_rate=0.08, lower_rate=0.05)
+    seqs += [b"A" * 30 + b"N" + b"C" * 30, b"a" * 31, b"ACGTN" * 20, b"", b"G" * 31 + b"N"]
+    data, offsets = scb.pack_sequences(seqs)
+    k = 31
+
+    def indexed(s: bytes) -> bool:
+        run = 0
+        for c in s:
+            run = run + 1 if chr(c) in "ACGTacgt" else 0
+            if run >= k:
+                return True
+        return False
+
+    b = scb.SuperCountingBloomBuilder(_cfg(scb, 31, 21, 25, 4, 20, 9, 16))
+    rep = b.add_sequences(data, offsets)
+    assert rep.records_indexed == sum(indexed(s) for s in seqs)
+    assert rep.records_processed == len(seqs)
