@@ -65,20 +65,28 @@ def parse():
 
 
 class Dist:
+    """One process per GPU (torchrun): NCCL over the GPUs, or gloo on a host without one (the
+    reference arm and the CPU tests of this launch path)."""
+
     def __init__(self, gpus: int):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
         self.pg = None
+        self.dev = "cpu"
         if self.world > 1:
             import datetime
 
             import torch
             import torch.distributed as dist
 
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                    device_id=torch.device("cuda", self.local))
+            timeout = datetime.timedelta(seconds=600)
+            if torch.cuda.is_available():
+                torch.cuda.set_device(self.local)
+                dist.init_process_group("nccl", timeout=timeout, device_id=torch.device("cuda", self.local))
+                self.dev = "cuda"
+            else:
+                dist.init_process_group("gloo", timeout=timeout)
             self.pg = dist
 
     def barrier(self):
@@ -90,7 +98,7 @@ class Dist:
             return v
         import torch
 
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        t = torch.tensor([v], dtype=torch.float64, device=self.dev)
         self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
         return float(t.item())
 
@@ -99,7 +107,7 @@ class Dist:
             return v
         import torch
 
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        t = torch.tensor([v], dtype=torch.float64, device=self.dev)
         self.pg.all_reduce(t, op=self.pg.ReduceOp.SUM)
         return float(t.item())
 

@@ -85,9 +85,26 @@ void fill_geometry(scb_ctx* ctx) {
 
 scb_status check_offsets(const uint64_t* offsets, uint64_t n) {
     if (!offsets) return fail_kind(SCB_ERR_INTERNAL_STATE, "null offsets");
-    // branch-free, so the compiler vectorises it: millions of offsets in a few milliseconds
+    // branch-free (vectorised) and, for millions of sequences, split over host threads: one
+    // thread streams offsets at about 10 GB/s, which alone would cost ~10 ms per 13 M reads
+    auto scan = [offsets](uint64_t a, uint64_t b) {
+        uint64_t bad = 0;
+        for (uint64_t i = a; i < b; i++) bad |= (uint64_t)(offsets[i + 1] < offsets[i]);
+        return bad;
+    };
+    const uint64_t parts = n < (1u << 20) ? 1 : std::min<uint64_t>(8, std::max(1u, std::thread::hardware_concurrency()));
     uint64_t bad = 0;
-    for (uint64_t i = 0; i < n; i++) bad |= (uint64_t)(offsets[i + 1] < offsets[i]);
+    if (parts == 1) {
+        bad = scan(0, n);
+    } else {
+        std::vector<uint64_t> res(parts, 0);
+        std::vector<std::thread> th;
+        for (uint64_t t = 0; t < parts; t++) {
+            th.emplace_back([&, t] { res[t] = scan(n * t / parts, n * (t + 1) / parts); });
+        }
+        for (auto& x : th) x.join();
+        for (uint64_t r : res) bad |= r;
+    }
     if (bad) return fail_kind(SCB_ERR_INTERNAL_STATE, "offsets must be non-decreasing");
     return SCB_OK;
 }
