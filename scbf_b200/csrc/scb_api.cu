@@ -276,15 +276,19 @@ uint32_t bucket_shift_for(const scb_ctx* ctx, uint64_t records) {
 // Sizes of the grouped pipeline for a batch: bucket shift and count, record slots (the estimate
 // with a quarter of slack, at least min_records, plus the unused tail of each CTA's last reserved
 // chunk of 4096 slots) and the work-item bound for that many records.
+// Sizes of the grouped pipeline for a batch: bucket shift and count; each bucket's region of
+// bucket_cap record slots (1.5x the expected records per bucket plus 64, rounded to a 32-byte
+// sector); the overflow list's capacity cap (records past their region: a quarter of the
+// estimate plus 64 Ki, at least min_records); and the work-item bound.
 struct GroupedSizes {
     uint32_t shift = 0;
-    uint64_t n_buckets = 0, cap = 0, max_items = 0;
+    uint64_t n_buckets = 0, bucket_cap = 0, cap = 0, max_items = 0;
+    uint64_t region() const { return n_buckets * bucket_cap; }
 };
 
-uint64_t chunk_tails(const scb_ctx* ctx) { return (uint64_t)(ctx->sm_count * 16 + 64) * 4096; }
-
-uint64_t items_bound(uint64_t n_buckets, uint64_t records) {
-    return std::min<uint64_t>(n_buckets, records) + records / kItemRecords + 1;
+uint64_t items_bound(const GroupedSizes& z) {
+    return z.n_buckets * ((z.bucket_cap + kItemRecords - 1) / kItemRecords) + std::min<uint64_t>(z.n_buckets, z.cap) +
+           z.cap / kItemRecords + 1;
 }
 
 // Probe slots kept between the insert and the query of the same records: one 64-bit word per
@@ -314,12 +318,15 @@ GroupedSizes grouped_sizes(const scb_ctx* ctx, uint64_t n_bytes, uint64_t min_re
     const uint64_t est = records_estimate(ctx, n_bytes);
     z.shift = bucket_shift_for(ctx, est);
     z.n_buckets = ctx->nb_blocks >> z.shift;
-    z.cap = std::max<uint64_t>(est * 5 / 4, min_records) + chunk_tails(ctx);
-    z.max_items = items_bound(z.n_buckets, z.cap);
+    z.bucket_cap = ((est / z.n_buckets * 3 / 2 + 64) + 3) & ~3ull;
+    z.cap = std::max<uint64_t>(est / 4 + 65536, min_records);
+    z.max_items = items_bound(z);
     return z;
 }
 
-scb_status grouped_buffers(Lane& L, const GroupedSizes& z, uint64_t sorted_records) {
+scb_status grouped_buffers(Lane& L, const GroupedSizes& z) {
+    if (z.region() + z.cap >= (1ull << 32))
+        return fail_kind(SCB_ERR_INTERNAL_STATE, "super-k-mer record slots beyond 2^32 for one batch");
     SCB_TRY(L.bhist.ensure((z.n_buckets + 1) * 8));
     SCB_TRY(L.bcursor.ensure((z.n_buckets + 1) * 8));
     SCB_TRY(L.icount.ensure((z.n_buckets + 1) * 8));
@@ -327,21 +334,23 @@ scb_status grouped_buffers(Lane& L, const GroupedSizes& z, uint64_t sorted_recor
     SCB_TRY(L.rec_count.ensure(64));
     SCB_TRY(L.rec_key.ensure(z.cap * 4));
     SCB_TRY(L.rec_val.ensure(z.cap * 8));
-    SCB_TRY(L.rec_sorted.ensure(std::max<uint64_t>(sorted_records, 1) * 8));
+    SCB_TRY(L.rec_sorted.ensure((z.region() + z.cap) * 8));
     SCB_TRY(L.items.ensure(z.max_items * 16));
     return SCB_OK;
 }
 
-// The cut kernel: one record per super-k-mer into slots [0, z.cap) and the bucket histogram.
+// The cut kernel: one record per super-k-mer, into its bucket's region or the overflow list.
 scb_status launch_cut(scb_ctx* ctx, Lane& L, TileArgs& a, const GroupedSizes& z, cudaStream_t st) {
     SCB_CUDA(cudaMemsetAsync(L.bhist.p, 0, (z.n_buckets + 1) * 8, st));
-    SCB_CUDA(cudaMemsetAsync(L.rec_count.p, 0, 16, st));  // record slots, probe slots
+    SCB_CUDA(cudaMemsetAsync(L.rec_count.p, 0, 16, st));  // overflow records, probe slots
     a.rec_key = L.rec_key.as<uint32_t>();
     a.rec_val = L.rec_val.as<unsigned long long>();
     a.rec_count = L.rec_count.as<unsigned long long>();
     a.rec_cap = z.cap;
     a.bucket_hist = L.bhist.as<unsigned long long>();
     a.bucket_shift = z.shift;
+    a.sorted = L.rec_sorted.as<unsigned long long>();
+    a.bucket_cap = z.bucket_cap;
     if (a.n_tiles == 0) return SCB_OK;
     SCB_CUDA(cudaMemsetAsync(L.tiles.p, 0, 4, st));
     launch_tiles(kModeCut, a, tile_grid(kModeCut, ctx->g.bits, ctx->sm_count, a.n_tiles), st);
@@ -349,19 +358,23 @@ scb_status launch_cut(scb_ctx* ctx, Lane& L, TileArgs& a, const GroupedSizes& z,
     return SCB_OK;
 }
 
-// Bucket offsets, the scatter of the records into bucket order and the work items.  Every
-// kernel here leaves the records alone when the cut reserved more than z.cap slots.
+// Work items over the bucket regions and the overflow records, which are first sorted into
+// bucket order after the regions.  Every kernel here leaves the records alone when the overflow
+// list ran out of room (more than z.cap entries).
 scb_status launch_bucketing(scb_ctx* ctx, Lane& L, const GroupedSizes& z, cudaStream_t st) {
     (void)ctx;
-    unsigned long long* hist = L.bhist.as<unsigned long long>();
-    launch_scan_inplace(reinterpret_cast<uint64_t*>(hist), z.n_buckets + 1, L.gscan.as<uint64_t>(), st);
-    SCB_CUDA(cudaMemcpyAsync(L.bcursor.p, L.bhist.p, (z.n_buckets + 1) * 8, cudaMemcpyDeviceToDevice, st));
+    const unsigned long long* counts = L.bhist.as<unsigned long long>();
+    uint64_t* ovf = reinterpret_cast<uint64_t*>(L.bcursor.p);
+    launch_item_counts(counts, z.n_buckets, z.bucket_cap, L.icount.as<uint64_t>(), ovf,
+                       L.rec_count.as<unsigned long long>(), z.cap, st);
+    launch_scan_inplace(L.icount.as<uint64_t>(), z.n_buckets + 1, L.gscan.as<uint64_t>(), st);
+    launch_scan_inplace(ovf, z.n_buckets + 1, L.gscan.as<uint64_t>(), st);
+    launch_item_write(counts, z.bucket_cap, L.icount.as<uint64_t>(), ovf, z.region(), z.n_buckets,
+                      L.items.as<uint4>(), st);
+    // the overflow cursors start at the overflow offsets, which item_write has read
     launch_scatter(L.rec_key.as<uint32_t>(), L.rec_val.as<unsigned long long>(),
                    L.rec_count.as<unsigned long long>(), z.cap, z.shift, L.bcursor.as<unsigned long long>(),
-                   L.rec_sorted.as<unsigned long long>(), st);
-    launch_item_counts(hist, z.n_buckets, L.icount.as<uint64_t>(), L.rec_count.as<unsigned long long>(), z.cap, st);
-    launch_scan_inplace(L.icount.as<uint64_t>(), z.n_buckets + 1, L.gscan.as<uint64_t>(), st);
-    launch_item_write(hist, L.icount.as<uint64_t>(), z.n_buckets, L.items.as<uint4>(), st);
+                   z.region(), L.rec_sorted.as<unsigned long long>(), st);
     SCB_CUDA(cudaGetLastError());
     return SCB_OK;
 }
@@ -426,13 +439,10 @@ scb_status grouped_prepare(scb_ctx* ctx, Lane& L, TileArgs& a, cudaStream_t st) 
     GroupedState& gs = L.gs;
     gs.valid = false;
     GroupedSizes z = grouped_sizes(ctx, a.n_bytes, 0);
-    unsigned long long produced = 0;
+    unsigned long long overflow = 0, records = 0;
     SCB_TRY(mark(ctx, L, 4, st));
     for (int attempt = 0; attempt < 2; attempt++) {
-        SCB_TRY(L.rec_key.ensure(z.cap * 4));
-        SCB_TRY(L.rec_val.ensure(z.cap * 8));
-        SCB_TRY(L.bhist.ensure((z.n_buckets + 1) * 8));
-        SCB_TRY(L.rec_count.ensure(64));
+        SCB_TRY(grouped_buffers(L, z));
         if (attempt == 1) {  // the cut's own counters only (windows, s-mers, super-k-mers)
             SCB_CUDA(cudaMemsetAsync(a.cnt + kCntWindows, 0, 8, st));
             SCB_CUDA(cudaMemsetAsync(a.cnt + kCntSmers, 0, 8, st));
@@ -440,25 +450,25 @@ scb_status grouped_prepare(scb_ctx* ctx, Lane& L, TileArgs& a, cudaStream_t st) 
         }
         SCB_TRY(launch_cut(ctx, L, a, z, st));
         SCB_TRY(mark(ctx, L, 5, st));
-        SCB_CUDA(cudaMemcpyAsync(&produced, L.rec_count.p, 8, cudaMemcpyDeviceToHost, st));
+        SCB_CUDA(cudaMemcpyAsync(&overflow, L.rec_count.p, 8, cudaMemcpyDeviceToHost, st));
+        SCB_CUDA(cudaMemcpyAsync(&records, a.cnt + kCntSuperKmers, 8, cudaMemcpyDeviceToHost, st));
         SCB_CUDA(cudaStreamSynchronize(st));
-        if (produced <= z.cap) break;
-        // more record slots than estimated: the count is exact up to the unused chunk tails of
-        // each CTA, so this capacity always suffices for the second cut
-        z.cap = produced + chunk_tails(ctx);
+        if (overflow <= z.cap) break;
+        // more records past their bucket's region than the list held: the count is exact, so
+        // a second cut with room for all of them suffices
+        z.cap = overflow + 65536;
+        z.max_items = items_bound(z);
     }
-    if (produced > z.cap) return fail_kind(SCB_ERR_INTERNAL_STATE, "super-k-mer record overflow");
-    gs.produced = produced;
+    if (overflow > z.cap) return fail_kind(SCB_ERR_INTERNAL_STATE, "super-k-mer record overflow");
+    gs.produced = records;
     gs.shift = z.shift;
     gs.n_buckets = z.n_buckets;
-    z.max_items = items_bound(z.n_buckets, produced);
-    gs.max_items = produced ? z.max_items : 0;
-    SCB_TRY(grouped_buffers(L, z, produced));
-    if (produced) SCB_TRY(launch_bucketing(ctx, L, z, st));
+    gs.max_items = records ? z.max_items : 0;
+    if (records) SCB_TRY(launch_bucketing(ctx, L, z, st));
     gs.ga = group_args(ctx, L, a, z);
     gs.probes_written = false;
     gs.probe_cap = 0;
-    if (L.want_probes && produced) {
+    if (L.want_probes && records) {
         gs.probe_cap = probe_capacity(ctx, a.n_bytes);
         SCB_TRY(L.probes.ensure(gs.probe_cap * 8));
         SCB_TRY(L.item_base.ensure(z.max_items * 8));
@@ -617,6 +627,7 @@ scb_status record_batch(scb_ctx* ctx, Lane& L, const GraphKey& K, cudaStream_t s
     z.shift = K.shift;
     z.n_buckets = K.n_buckets;
     z.cap = K.rec_cap;
+    z.bucket_cap = K.bucket_cap;
     z.max_items = K.max_items;
     bool cut = K.kind == kBatchReportKept;  // the insert's records are kept
     auto cut_and_bucket = [&]() -> scb_status {
@@ -739,9 +750,10 @@ scb_status graph_launch(scb_ctx* ctx, Lane& L, int kind, const uint8_t* d_ascii,
             K.shift = z.shift;
             K.n_buckets = z.n_buckets;
             K.rec_cap = z.cap;
+            K.bucket_cap = z.bucket_cap;
             K.max_items = z.max_items;
             K.apply_threads = ctx->tuning.apply_threads;
-            SCB_TRY(grouped_buffers(L, z, z.cap));
+            SCB_TRY(grouped_buffers(L, z));
             const bool keep = kind == kBatchInsertKeep ||
                               (kind == kBatchBuildStream && K.s_ins == SCB_STRATEGY_GROUPED &&
                                K.s_query == SCB_STRATEGY_GROUPED);

@@ -137,12 +137,13 @@ inline bool kind_queries(int kind) { return kind == kBatchReport || kind == kBat
 // sizes, plus a signature of the lane buffers the graph's nodes point at.
 struct GraphKey {
     int kind = 0, s_ins = 0, s_query = 0;
-    uint64_t cap_bytes = 0, rec_cap = 0, max_items = 0, n_buckets = 0, probe_cap = 0;
+    uint64_t cap_bytes = 0, rec_cap = 0, bucket_cap = 0, max_items = 0, n_buckets = 0, probe_cap = 0;
     uint32_t shift = 0, apply_threads = 0;
     uint64_t sig = 0;
     bool operator==(const GraphKey& o) const {
         return kind == o.kind && s_ins == o.s_ins && s_query == o.s_query &&
-               cap_bytes == o.cap_bytes && rec_cap == o.rec_cap && probe_cap == o.probe_cap &&
+               cap_bytes == o.cap_bytes && rec_cap == o.rec_cap && bucket_cap == o.bucket_cap &&
+               probe_cap == o.probe_cap &&
                max_items == o.max_items && n_buckets == o.n_buckets && shift == o.shift &&
                apply_threads == o.apply_threads && sig == o.sig;
     }

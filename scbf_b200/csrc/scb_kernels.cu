@@ -333,14 +333,9 @@ struct TileSmem {
     uint32_t n_ends;
     uint32_t tile;
     uint64_t seq_lo, seq_hi;
-    // cut mode: record slots reserved by this CTA in chunks (one global atomic per chunk)
-    uint64_t chunk_base, tile_base;
-    uint32_t chunk_used, chunk_cap;
     uint32_t warp_cnt[kTileThreads / 32];
 };
 
-constexpr uint32_t kRecChunk = 4096;                // record slots reserved per global atomic
-constexpr unsigned long long kRecInvalid = ~0ull;  // unused reserved slot
 
 // Fills the per-CTA ntHash tables for m-mers of length m:
 //   nt3f[c][x] = XOR over bases t of chunk c of rotl(seed(base), 7 * (m - 1 - (3c + t)))
@@ -496,11 +491,6 @@ __global__ void __launch_bounds__(kTileThreads, 8) k_tiles(TileArgs a) {
         n_tiles = (uint32_t)((n_bytes + kTileWindows - 1) / kTileWindows);
     }
     fill_nt_tables(sm, g.m);
-    if (MODE == kModeCut && tid == 0) {
-        sm.chunk_base = 0;
-        sm.chunk_used = 0;
-        sm.chunk_cap = 0;
-    }
 
     while (true) {
         if (tid == 0) sm.tile = atomicAdd(a.tile_counter, 1u);
@@ -699,7 +689,6 @@ __global__ void __launch_bounds__(kTileThreads, 8) k_tiles(TileArgs a) {
             }
         } else if constexpr (MODE == kModeCut) {
             // one record per super-k-mer, emitted at its last window: (block, first window, windows).
-            // Slots: thread-contiguous within the tile, the tile's run taken from this CTA's chunk.
             constexpr uint32_t kPer = kTileWindows / kTileThreads;
             const uint32_t lane = tid & 31, wid = tid >> 5;
             uint32_t mine = 0;  // ends among this thread's windows back + tid*kPer .. + kPer - 1
@@ -729,30 +718,10 @@ __global__ void __launch_bounds__(kTileThreads, 8) k_tiles(TileArgs a) {
                 const uint16_t po = sm.poff[i];
                 if (po != kNoWindow && sm.poff[i + 1] != po) sm.ends[before++] = (uint16_t)i;
             }
-            if (tid == 0) {
-                if (sm.chunk_used + tile_total > sm.chunk_cap) {
-                    // retire the rest of the current chunk (marked below) and reserve a new one
-                    const uint32_t want = tile_total > kRecChunk ? tile_total : kRecChunk;
-                    sm.tile_base = sm.chunk_base + sm.chunk_used;  // start of the retired rest
-                    sm.n_ends = sm.chunk_cap - sm.chunk_used;      // its length
-                    sm.chunk_base = atomicAdd(a.rec_count, (unsigned long long)want);
-                    sm.chunk_cap = want;
-                    sm.chunk_used = 0;
-                } else {
-                    sm.n_ends = 0;
-                }
-            }
             __syncthreads();
-            for (uint32_t x = tid; x < sm.n_ends; x += blockDim.x) {
-                const unsigned long long slot = sm.tile_base + x;
-                if (slot < a.rec_cap) a.rec_val[slot] = kRecInvalid;
-            }
-            __syncthreads();
-            if (tid == 0) {
-                sm.tile_base = sm.chunk_base + sm.chunk_used;
-                sm.chunk_used += tile_total;
-            }
-            __syncthreads();
+            // each record takes the next slot of its bucket's region; past the region it goes to
+            // the overflow list (sorted into place by the bucketing step)
+            const uint32_t local_mask = (1u << a.bucket_shift) - 1u;
             for (uint32_t e = tid; e < tile_total; e += blockDim.x) {
                 const uint32_t i = sm.ends[e];
                 const uint16_t po = sm.poff[i];
@@ -762,12 +731,20 @@ __global__ void __launch_bounds__(kTileThreads, 8) k_tiles(TileArgs a) {
                 c_sk++;
                 c_smer += nwin + ks;
                 const uint32_t block = minimizer_block(sm.codes, e0 + po - cb, g);
-                const unsigned long long slot = sm.tile_base + e;
-                if (slot < a.rec_cap) {
-                    a.rec_key[slot] = block;
-                    a.rec_val[slot] = (unsigned long long)(e0 + st) | ((unsigned long long)nwin << kRecWindowsShift);
+                const unsigned long long val =
+                    (unsigned long long)(e0 + st) | ((unsigned long long)nwin << kRecWindowsShift);
+                const uint32_t bucket = block >> a.bucket_shift;
+                const unsigned long long slot = atomicAdd(a.bucket_hist + bucket, 1ull);
+                if (slot < a.bucket_cap) {
+                    a.sorted[(uint64_t)bucket * a.bucket_cap + slot] =
+                        val | ((unsigned long long)(block & local_mask) << kRecLocalShift);
+                } else {
+                    const unsigned long long o = atomicAdd(a.rec_count, 1ull);
+                    if (o < a.rec_cap) {
+                        a.rec_key[o] = block;
+                        a.rec_val[o] = val;
+                    }
                 }
-                atomicAdd(a.bucket_hist + (block >> a.bucket_shift), 1ull);
             }
         } else if constexpr (MODE == kModeDebugMin) {
             for (uint32_t i = tid; i < kTileWindows; i += blockDim.x) {
@@ -784,14 +761,6 @@ __global__ void __launch_bounds__(kTileThreads, 8) k_tiles(TileArgs a) {
             }
         }
         __syncthreads();
-    }
-    if constexpr (MODE == kModeCut) {
-        // mark the unused rest of this CTA's last chunk (the loop ended after a barrier)
-        const uint64_t rest0 = sm.chunk_base + sm.chunk_used;
-        const uint32_t rest = sm.chunk_cap - sm.chunk_used;
-        for (uint32_t x = tid; x < rest; x += blockDim.x) {
-            if (rest0 + x < a.rec_cap) a.rec_val[rest0 + x] = kRecInvalid;
-        }
     }
     warp_add_u64(&a.cnt[kCntWindows], c_win);
     warp_add_u64(&a.cnt[kCntSmers], c_smer);
@@ -1013,47 +982,61 @@ void launch_counter_hist(const void* table, uint64_t slots, int bits, unsigned l
 // ---------------------------------------------------------------------------------------
 // Grouped pipeline: records bucketed by block; each work item's blocks live in shared memory.
 // ---------------------------------------------------------------------------------------
+// Overflow records (those past their bucket's region) into bucket order after the regions:
+// position = base + the bucket's overflow offset + its running count.
 __global__ void k_scatter(const uint32_t* __restrict__ key, const unsigned long long* __restrict__ val,
                           const unsigned long long* __restrict__ count, uint64_t cap, uint32_t shift,
-                          unsigned long long* __restrict__ cursor, unsigned long long* __restrict__ sorted) {
+                          unsigned long long* __restrict__ cursor, uint64_t base,
+                          unsigned long long* __restrict__ sorted) {
     const uint64_t n = *count;
-    if (n > cap) return;  // the cut ran out of record slots: the host redoes the batch
+    if (n > cap) return;  // the overflow list ran out of room: the host redoes the batch
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     const uint32_t local_mask = (1u << shift) - 1u;
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const unsigned long long v = val[i];
-        if (v == kRecInvalid) continue;  // unused slot of a reserved chunk
         const uint32_t block = key[i];
-        const unsigned long long pos = atomicAdd(cursor + (block >> shift), 1ull);
+        const unsigned long long pos = base + atomicAdd(cursor + (block >> shift), 1ull);
         sorted[pos] = v | ((unsigned long long)(block & local_mask) << kRecLocalShift);
     }
 }
 
-__global__ void k_item_counts(const unsigned long long* __restrict__ off, uint64_t n_buckets,
-                              uint64_t* __restrict__ item_count, const unsigned long long* __restrict__ rec_count,
-                              uint64_t rec_cap) {
+// Work items per bucket: its region's records (at most bucket_cap) and its overflow records, in
+// items of at most kItemRecords; also each bucket's overflow count (for the overflow offsets).
+__global__ void k_item_counts(const unsigned long long* __restrict__ counts, uint64_t n_buckets, uint64_t bucket_cap,
+                              uint64_t* __restrict__ item_count, uint64_t* __restrict__ ovf_count,
+                              const unsigned long long* __restrict__ rec_count, uint64_t rec_cap) {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     const bool overflow = *rec_count > rec_cap;  // no work items: nothing is applied
     for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; b <= n_buckets; b += stride) {
         if (b == n_buckets || overflow) {
             item_count[b] = 0;
+            ovf_count[b] = 0;
         } else {
-            const uint64_t c = off[b + 1] - off[b];
-            item_count[b] = (c + kItemRecords - 1) / kItemRecords;
+            const uint64_t c = counts[b];
+            const uint64_t m = c < bucket_cap ? c : bucket_cap, o = c - m;
+            item_count[b] = (m + kItemRecords - 1) / kItemRecords + (o + kItemRecords - 1) / kItemRecords;
+            ovf_count[b] = o;
         }
     }
 }
 
-__global__ void k_item_write(const unsigned long long* __restrict__ off, const uint64_t* __restrict__ item_off,
-                             uint64_t n_buckets, uint4* __restrict__ items) {
+__global__ void k_item_write(const unsigned long long* __restrict__ counts, uint64_t bucket_cap,
+                             const uint64_t* __restrict__ item_off, const uint64_t* __restrict__ ovf_off,
+                             uint64_t ovf_base, uint64_t n_buckets, uint4* __restrict__ items) {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; b < n_buckets; b += stride) {
-        const uint64_t c = off[b + 1] - off[b];
-        const uint64_t ni = item_off[b + 1] - item_off[b];
-        for (uint64_t t = 0; t < ni; t++) {
-            const uint64_t first = off[b] + t * kItemRecords;
-            const uint64_t cnt = min((uint64_t)kItemRecords, c - t * kItemRecords);
-            items[item_off[b] + t] = make_uint4((uint32_t)b, (uint32_t)first, (uint32_t)cnt, ni == 1 ? 1u : 0u);
+        const uint64_t c = counts[b];
+        const uint64_t m = c < bucket_cap ? c : bucket_cap, o = c - m;
+        const uint64_t i0 = item_off[b];
+        const uint32_t excl = item_off[b + 1] - i0 == 1 ? 1u : 0u;  // the bucket's only item
+        uint64_t t = 0;
+        for (uint64_t r = 0; r < m; r += kItemRecords, t++) {
+            const uint64_t cnt = min((uint64_t)kItemRecords, m - r);
+            items[i0 + t] = make_uint4((uint32_t)b, (uint32_t)(b * bucket_cap + r), (uint32_t)cnt, excl);
+        }
+        for (uint64_t r = 0; r < o; r += kItemRecords, t++) {
+            const uint64_t cnt = min((uint64_t)kItemRecords, o - r);
+            items[i0 + t] = make_uint4((uint32_t)b, (uint32_t)(ovf_base + ovf_off[b] + r), (uint32_t)cnt, excl);
         }
     }
 }
@@ -1508,27 +1491,29 @@ void launch_apply(int mode, const GroupArgs& a, int bs_log2, uint32_t bucket_blo
 }
 
 void launch_scatter(const uint32_t* rec_key, const unsigned long long* rec_val, const unsigned long long* rec_count,
-                    uint64_t rec_cap, uint32_t bucket_shift, unsigned long long* cursor, unsigned long long* sorted,
-                    cudaStream_t st) {
+                    uint64_t rec_cap, uint32_t bucket_shift, unsigned long long* cursor, uint64_t base,
+                    unsigned long long* sorted, cudaStream_t st) {
     const uint64_t blocks = (rec_cap + 255) / 256;
-    k_scatter<<<(unsigned)(blocks < 16384 ? (blocks ? blocks : 1) : 16384), 256, 0, st>>>(
-        rec_key, rec_val, rec_count, rec_cap, bucket_shift, cursor, sorted);
+    k_scatter<<<(unsigned)(blocks < 4096 ? (blocks ? blocks : 1) : 4096), 256, 0, st>>>(
+        rec_key, rec_val, rec_count, rec_cap, bucket_shift, cursor, base, sorted);
     note_launch();
 }
 
-void launch_item_counts(const unsigned long long* bucket_off, uint64_t n_buckets, uint64_t* item_count,
-                        const unsigned long long* rec_count, uint64_t rec_cap, cudaStream_t st) {
+void launch_item_counts(const unsigned long long* counts, uint64_t n_buckets, uint64_t bucket_cap, uint64_t* item_count,
+                        uint64_t* ovf_count, const unsigned long long* rec_count, uint64_t rec_cap, cudaStream_t st) {
     const uint64_t blocks = (n_buckets + 1 + 255) / 256;
-    k_item_counts<<<(unsigned)(blocks < 16384 ? blocks : 16384), 256, 0, st>>>(bucket_off, n_buckets, item_count,
-                                                                              rec_count, rec_cap);
+    k_item_counts<<<(unsigned)(blocks < 16384 ? blocks : 16384), 256, 0, st>>>(counts, n_buckets, bucket_cap,
+                                                                              item_count, ovf_count, rec_count,
+                                                                              rec_cap);
     note_launch();
 }
 
-void launch_item_write(const unsigned long long* bucket_off, const uint64_t* item_off, uint64_t n_buckets,
-                       uint4* items, cudaStream_t st) {
+void launch_item_write(const unsigned long long* counts, uint64_t bucket_cap, const uint64_t* item_off,
+                       const uint64_t* ovf_off, uint64_t ovf_base, uint64_t n_buckets, uint4* items,
+                       cudaStream_t st) {
     const uint64_t blocks = (n_buckets + 255) / 256;
-    k_item_write<<<(unsigned)(blocks < 16384 ? (blocks ? blocks : 1) : 16384), 256, 0, st>>>(bucket_off, item_off,
-                                                                                           n_buckets, items);
+    k_item_write<<<(unsigned)(blocks < 16384 ? (blocks ? blocks : 1) : 16384), 256, 0, st>>>(
+        counts, bucket_cap, item_off, ovf_off, ovf_base, n_buckets, items);
     note_launch();
 }
 

@@ -38,7 +38,7 @@ struct BatchParams {
 };
 
 // Grouped pipeline: super-k-mer records bucketed by counter block.
-// Unsorted record: key = block id, val = first window position | windows << 32.
+// Overflow record: key = block id, val = first window position | windows << 32.
 // Sorted record:   val = first window position | windows << 32 | block-in-bucket << 38.
 constexpr uint32_t kRecWindowsShift = 32;
 constexpr uint32_t kRecLocalShift = 38;
@@ -124,7 +124,9 @@ struct TileArgs {
     uint32_t* wblock;
     uint8_t* wend;
     uint32_t* dbg;
-    // grouped pipeline (kModeCut)
+    // grouped pipeline (kModeCut): records go to their bucket's region of bucket_cap slots in
+    // sorted (bucket_hist counts them per bucket), the rest to the overflow list rec_key / rec_val
+    // of rec_cap entries (rec_count counts them)
     uint32_t* rec_key;
     unsigned long long* rec_val;
     unsigned long long* rec_count;
@@ -132,6 +134,8 @@ struct TileArgs {
     unsigned long long* bucket_hist;
     uint32_t bucket_shift;
     uint32_t pad3_;
+    unsigned long long* sorted;
+    uint64_t bucket_cap;
     // when set, n_bytes / n_seqs / offsets come from here at run time (graph replays) and the
     // fields above give the capacity of the batch's shape class
     const BatchParams* dyn;
@@ -164,12 +168,13 @@ void launch_counter_hist(const void* table, uint64_t slots, int bits, unsigned l
 void launch_fill_u32(uint32_t* p, uint32_t v, uint64_t n, cudaStream_t st);
 // grouped pipeline
 void launch_scatter(const uint32_t* rec_key, const unsigned long long* rec_val, const unsigned long long* rec_count,
-                    uint64_t rec_cap, uint32_t bucket_shift, unsigned long long* cursor, unsigned long long* sorted,
-                    cudaStream_t st);
-void launch_item_counts(const unsigned long long* bucket_off, uint64_t n_buckets, uint64_t* item_count,
-                        const unsigned long long* rec_count, uint64_t rec_cap, cudaStream_t st);
-void launch_item_write(const unsigned long long* bucket_off, const uint64_t* item_off, uint64_t n_buckets,
-                       uint4* items, cudaStream_t st);
+                    uint64_t rec_cap, uint32_t bucket_shift, unsigned long long* cursor, uint64_t base,
+                    unsigned long long* sorted, cudaStream_t st);
+void launch_item_counts(const unsigned long long* counts, uint64_t n_buckets, uint64_t bucket_cap, uint64_t* item_count,
+                        uint64_t* ovf_count, const unsigned long long* rec_count, uint64_t rec_cap, cudaStream_t st);
+void launch_item_write(const unsigned long long* counts, uint64_t bucket_cap, const uint64_t* item_off,
+                       const uint64_t* ovf_off, uint64_t ovf_base, uint64_t n_buckets, uint4* items,
+                       cudaStream_t st);
 void launch_apply(int mode, const GroupArgs& a, int block_slots, uint32_t bucket_blocks, int sm_count,
                   uint64_t max_items, cudaStream_t st);
 
