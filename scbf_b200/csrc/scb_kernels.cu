@@ -1137,7 +1137,10 @@ constexpr uint32_t kProbeBatch = 4;
 
 __host__ __device__ inline uint32_t align16(uint32_t x) { return (x + 15u) & ~15u; }
 
-__host__ __device__ inline ApplyLayout apply_layout(int mode, int bits, uint32_t bucket_slots, uint32_t bucket_blocks) {
+// lean: a query over kept probe slots stages no bases (items without slots read the codes from
+// global memory), which leaves room for more CTAs per SM.
+__host__ __device__ inline ApplyLayout apply_layout(int mode, int bits, uint32_t bucket_slots, uint32_t bucket_blocks,
+                                                    bool lean = false) {
     ApplyLayout l;
     const uint32_t cell_bytes = mode == kModeInsert ? 4u : (uint32_t)bits / 8u;
     const uint32_t max_smers = kSmerBudget, max_windows = kSmerBudget;
@@ -1146,8 +1149,8 @@ __host__ __device__ inline ApplyLayout apply_layout(int mode, int bits, uint32_t
     l.spre = l.rv + align16(kApplyChunk * 8u);
     l.wpre = l.spre + align16((kApplyChunk + 1u) * 4u);
     l.bases = l.wpre + align16((kApplyChunk + 1u) * 4u);
-    l.rbases = l.bases + align16(kApplyChunk * kRecBaseWords * 4u);
-    l.smap = l.rbases + align16(kApplyChunk * kRecBaseWords * 4u + 16u);  // + the last record's over-read
+    l.rbases = l.bases + (lean ? 0u : align16(kApplyChunk * kRecBaseWords * 4u));
+    l.smap = l.rbases + (lean ? 0u : align16(kApplyChunk * kRecBaseWords * 4u + 16u));  // + the last record's over-read
     l.wmap = l.smap + align16(max_smers);
     l.touched = l.wmap + (mode == kModeInsert ? 0u : align16(max_windows));
     l.est = l.touched + align16(bucket_blocks);
@@ -1158,7 +1161,7 @@ __host__ __device__ inline ApplyLayout apply_layout(int mode, int bits, uint32_t
 // NH = 4: four hashes per s-mer (the default geometry), unrolled; NH = 0: any n_hashes.  Kept
 // probe slots are 16-bit lanes (n_hashes <= 4), each the counter's index within the bucket's
 // shared-memory cells, so the query needs neither the s-mer nor its record.
-template <int MODE, int BITS, int NH>
+template <int MODE, int BITS, int NH, bool LEAN>
 __device__ __forceinline__ void apply_body(const GroupArgs& a, uint32_t bs_log2, uint32_t bucket_blocks) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     using T = CounterTraits<BITS>;
@@ -1168,7 +1171,7 @@ __device__ __forceinline__ void apply_body(const GroupArgs& a, uint32_t bs_log2,
     const DevGeom g = a.g;
     const uint32_t bs = 1u << bs_log2;
     const uint32_t bucket_slots = bs * bucket_blocks;
-    const ApplyLayout lay = apply_layout(MODE, BITS, bucket_slots, bucket_blocks);
+    const ApplyLayout lay = apply_layout(MODE, BITS, bucket_slots, bucket_blocks, LEAN);
     Cell* cells = reinterpret_cast<Cell*>(smem_raw + lay.cells);
     unsigned long long* rv = reinterpret_cast<unsigned long long*>(smem_raw + lay.rv);
     uint32_t* spre = reinterpret_cast<uint32_t*>(smem_raw + lay.spre);
@@ -1263,7 +1266,7 @@ __device__ __forceinline__ void apply_body(const GroupArgs& a, uint32_t bs_log2,
             // stage the records' bases, kRecBaseWords consecutive threads per record (one sector
             // read, conflict-free shared stores), and their reverse complements (a query with the
             // insert's probe slots needs no bases)
-            for (uint32_t x = tid; x < (have_probes ? 0u : nuse * kRecBaseWords); x += blockDim.x) {
+            for (uint32_t x = tid; x < (have_probes || LEAN ? 0u : nuse * kRecBaseWords); x += blockDim.x) {
                 const uint32_t r = x / kRecBaseWords, j = x % kRecBaseWords;
                 const uint32_t cw = __ldg(a.codes + ((uint32_t)rv[r] >> 4) + j);
                 bases[x] = cw;
@@ -1325,9 +1328,15 @@ __device__ __forceinline__ void apply_body(const GroupArgs& a, uint32_t bs_log2,
                 // words: base t of it is the complement of forward base rel + s - 1 - t, which
                 // sits at position 16 * kRecBaseWords - rel - s + t of the mirrored stream (bits
                 // read past the record's words land above 2s and are masked off)
-                const uint64_t fw = codes64(bases + r * kRecBaseWords, rel) & s_mask;
-                const uint64_t rc = codes64(rbases + r * kRecBaseWords, 16u * kRecBaseWords - rel - g.s) & s_mask;
-                uint64_t hash = xorshift64(fw < rc ? fw : rc);
+                uint64_t smer;
+                if constexpr (LEAN) {  // no staged bases: the codes from global memory
+                    smer = canonical(codes64(a.codes, start + (f - spre[r])) & s_mask, g.s);
+                } else {
+                    const uint64_t fw = codes64(bases + r * kRecBaseWords, rel) & s_mask;
+                    const uint64_t rc = codes64(rbases + r * kRecBaseWords, 16u * kRecBaseWords - rel - g.s) & s_mask;
+                    smer = fw < rc ? fw : rc;
+                }
+                uint64_t hash = xorshift64(smer);
                 Cell* blk = cells + (lb << bs_log2);
                 if constexpr (MODE == kModeInsert) {
                     unsigned long long pk = 0;
@@ -1433,31 +1442,36 @@ __device__ __forceinline__ void apply_body(const GroupArgs& a, uint32_t bs_log2,
 template <int MODE, int BITS, int NH>
 __global__ void __launch_bounds__(kApplyMaxThreads) k_apply_insert(GroupArgs a, uint32_t bs_log2,
                                                                     uint32_t bucket_blocks) {
-    apply_body<MODE, BITS, NH>(a, bs_log2, bucket_blocks);
+    apply_body<MODE, BITS, NH, false>(a, bs_log2, bucket_blocks);
 }
 
 // The query is held to 2048 threads per SM at every CTA width (at most 32 registers), which
 // measured faster than the compiler's own choice; the insert measured faster without it.
-template <int MODE, int BITS, int NH>
+template <int MODE, int BITS, int NH, bool LEAN>
 __global__ void __launch_bounds__(kApplyMaxThreads, 2048 / kApplyMaxThreads) k_apply_query(GroupArgs a,
                                                                                            uint32_t bs_log2,
                                                                                            uint32_t bucket_blocks) {
-    apply_body<MODE, BITS, NH>(a, bs_log2, bucket_blocks);
+    apply_body<MODE, BITS, NH, LEAN>(a, bs_log2, bucket_blocks);
 }
 
-static size_t apply_smem(int mode, int bits, uint32_t bucket_slots, uint32_t bucket_blocks) {
-    return apply_layout(mode, bits, bucket_slots, bucket_blocks).total;
+static size_t apply_smem(int mode, int bits, uint32_t bucket_slots, uint32_t bucket_blocks, bool lean) {
+    return apply_layout(mode, bits, bucket_slots, bucket_blocks, lean).total;
 }
 
 template <int MODE, int BITS>
 static void launch_apply_t(const GroupArgs& a, int bs_log2, uint32_t bucket_blocks, int sm_count, uint64_t max_items,
                            cudaStream_t st) {
-    const size_t smem = apply_smem(MODE, BITS, (1u << bs_log2) * bucket_blocks, bucket_blocks);
+    const bool lean = MODE != kModeInsert && a.probes != nullptr;
+    const size_t smem = apply_smem(MODE, BITS, (1u << bs_log2) * bucket_blocks, bucket_blocks, lean);
     void (*fn)(GroupArgs, uint32_t, uint32_t);
     if constexpr (MODE == kModeInsert) {
         fn = a.g.h == 4 ? k_apply_insert<MODE, BITS, 4> : k_apply_insert<MODE, BITS, 0>;
     } else {
-        fn = a.g.h == 4 ? k_apply_query<MODE, BITS, 4> : k_apply_query<MODE, BITS, 0>;
+        if (lean) {
+            fn = a.g.h == 4 ? k_apply_query<MODE, BITS, 4, true> : k_apply_query<MODE, BITS, 0, true>;
+        } else {
+            fn = a.g.h == 4 ? k_apply_query<MODE, BITS, 4, false> : k_apply_query<MODE, BITS, 0, false>;
+        }
     }
     cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     // one thread per staged record at least (256 or 512 threads)
