@@ -1168,6 +1168,7 @@ __device__ __forceinline__ void apply_body(const GroupArgs& a, uint32_t bs_log2,
     using Cnt = typename CounterType<BITS>::type;
     using Cell = typename std::conditional<MODE == kModeInsert, uint32_t, Cnt>::type;
     using Est = typename std::conditional<(BITS <= 16), uint16_t, uint32_t>::type;
+    constexpr uint32_t kVecLog2 = BITS == 8 ? 4u : (BITS == 16 ? 3u : 2u);  // log2 counters per 16 bytes
     const DevGeom g = a.g;
     const uint32_t bs = 1u << bs_log2;
     const uint32_t bucket_slots = bs * bucket_blocks;
@@ -1240,18 +1241,37 @@ __device__ __forceinline__ void apply_body(const GroupArgs& a, uint32_t bs_log2,
 
         for (uint32_t x = tid; x < bucket_blocks; x += blockDim.x) touched[x] = 0;
         if constexpr (MODE == kModeInsert) {
-            for (uint32_t x = tid; x < bucket_slots; x += blockDim.x) cells[x] = 0;
+            if ((bucket_slots & 3u) == 0) {
+                uint4* c4 = reinterpret_cast<uint4*>(cells);
+                for (uint32_t x = tid; x < bucket_slots / 4; x += blockDim.x) c4[x] = make_uint4(0u, 0u, 0u, 0u);
+            } else {
+                for (uint32_t x = tid; x < bucket_slots; x += blockDim.x) cells[x] = 0;
+            }
         }
         __syncthreads();
         if constexpr (MODE == kModeReport) {
-            // stage the counters of the blocks this item reads
+            // stage the counters of the blocks this item reads, 16 bytes per load when a block
+            // holds at least that much
             for (uint32_t r = tid; r < count; r += blockDim.x) touched[a.recs[first + r] >> kRecLocalShift] = 1;
             __syncthreads();
-            for (uint32_t x = tid; x < bucket_slots; x += blockDim.x) {
-                const uint32_t lb = x >> bs_log2;
-                if (!touched[lb]) continue;
-                const uint64_t base = block_base(g, (bucket << a.bucket_shift) | lb);
-                cells[x] = (Cell)load_counter<BITS>(a.table, base + (x & (bs - 1)));
+            if (bs_log2 >= kVecLog2) {
+                const uint32_t vlog = bs_log2 - kVecLog2;
+                const uint32_t n_vec = bucket_blocks << vlog;
+                uint4* c4 = reinterpret_cast<uint4*>(cells);
+                for (uint32_t x = tid; x < n_vec; x += blockDim.x) {
+                    const uint32_t lb = x >> vlog;
+                    if (!touched[lb]) continue;
+                    const uint64_t base = block_base(g, (bucket << a.bucket_shift) | lb);
+                    const uint4* src = reinterpret_cast<const uint4*>(reinterpret_cast<const Cnt*>(a.table) + base);
+                    c4[x] = __ldg(src + (x & ((1u << vlog) - 1u)));
+                }
+            } else {
+                for (uint32_t x = tid; x < bucket_slots; x += blockDim.x) {
+                    const uint32_t lb = x >> bs_log2;
+                    if (!touched[lb]) continue;
+                    const uint64_t base = block_base(g, (bucket << a.bucket_shift) | lb);
+                    cells[x] = (Cell)load_counter<BITS>(a.table, base + (x & (bs - 1)));
+                }
             }
             __syncthreads();
         }
@@ -1275,6 +1295,7 @@ __device__ __forceinline__ void apply_body(const GroupArgs& a, uint32_t bs_log2,
             if (tid < nuse) {  // record index of its s-mers (not needed with kept slots) / windows
                 const uint32_t s0 = spre[tid], s1 = have_probes ? s0 : spre[tid + 1];
                 for (uint32_t f = s0; f < s1; f++) smap[f] = (uint8_t)tid;
+                if constexpr (MODE == kModeInsert) touched[(uint32_t)(rv[tid] >> kRecLocalShift)] = 1;
                 if constexpr (MODE == kModeReport) {
                     const uint32_t w0i = wpre[tid], w1i = wpre[tid + 1];
                     for (uint32_t vv = w0i; vv < w1i; vv++) wmap[vv] = (uint8_t)tid;
@@ -1361,7 +1382,6 @@ __device__ __forceinline__ void apply_body(const GroupArgs& a, uint32_t bs_log2,
                             hash = xorshift64(hash);
                         }
                     }
-                    touched[lb] = 1;
                     if (pbase != kNoProbes) __stcs(a.probes + pbase + poff + f, pk);
                 } else {
                     uint32_t e = T::kMax;
@@ -1405,7 +1425,43 @@ __device__ __forceinline__ void apply_body(const GroupArgs& a, uint32_t bs_log2,
             // commit the deltas: min(old + delta, MAX) per counter (counter.rs saturation)
             constexpr uint32_t lanes = T::kLanes;
             const bool word_ok = exclusive && (bs % lanes) == 0;
-            if (word_ok) {
+            if (exclusive && bs_log2 >= kVecLog2) {
+                // 16 bytes of the table per thread: kVec counters, their u32 deltas in shared memory
+                constexpr uint32_t kVec = 1u << kVecLog2;
+                const uint32_t vlog = bs_log2 - kVecLog2;
+                const uint32_t n_vec = bucket_blocks << vlog;
+                const uint4* d4 = reinterpret_cast<const uint4*>(cells);
+                for (uint32_t x = tid; x < n_vec; x += blockDim.x) {
+                    const uint32_t lb = x >> vlog;
+                    if (!touched[lb]) continue;
+                    const uint64_t base = block_base(g, (bucket << a.bucket_shift) | lb);
+                    uint4* wp = reinterpret_cast<uint4*>(reinterpret_cast<Cnt*>(a.table) + base) + (x & ((1u << vlog) - 1u));
+                    const uint4 o4 = __ldcg(wp);
+                    uint32_t d[kVec];
+#pragma unroll
+                    for (uint32_t q = 0; q < kVec / 4; q++) {
+                        const uint4 v = d4[x * (kVec / 4) + q];
+                        d[4 * q] = v.x;
+                        d[4 * q + 1] = v.y;
+                        d[4 * q + 2] = v.z;
+                        d[4 * q + 3] = v.w;
+                    }
+                    const uint32_t ow[4] = {o4.x, o4.y, o4.z, o4.w};
+                    uint32_t nw[4];
+#pragma unroll
+                    for (uint32_t w = 0; w < 4; w++) {
+                        uint32_t acc = 0;
+#pragma unroll
+                        for (uint32_t l = 0; l < lanes; l++) {
+                            const uint64_t cur = (ow[w] >> (l * BITS)) & T::kMax;
+                            const uint64_t sum = cur + d[w * lanes + l];
+                            acc |= (uint32_t)(sum < T::kMax ? sum : T::kMax) << (l * BITS);
+                        }
+                        nw[w] = acc;
+                    }
+                    __stcg(wp, make_uint4(nw[0], nw[1], nw[2], nw[3]));
+                }
+            } else if (word_ok) {
                 const uint32_t block_words = bs / lanes;
                 for (uint32_t x = tid; x < bucket_blocks * block_words; x += blockDim.x) {
                     const uint32_t lb = x / block_words, wi = x % block_words;
