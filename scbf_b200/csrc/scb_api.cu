@@ -125,19 +125,28 @@ struct Chunk {
     uint64_t win0;          // first output window of the chunk
 };
 
-// Pieces of whole sequences of at most cap bytes (one longer sequence alone), found by binary
-// search over the (validated, non-decreasing) offsets; win0 is not filled.
-scb_status plan_pieces(const uint64_t* offsets, uint64_t n, uint64_t cap, std::vector<Chunk>& out) {
+// Pieces of whole sequences for an upload pipeline: the first about cap / 1.3^3 bytes and each
+// next 1.3x larger, up to cap, so the first copy (which no work overlaps) is short while later
+// copies stay ahead of the work on the pieces before them; a tail under cap / 4 joins the piece
+// before it.  One longer sequence goes alone.
+scb_status plan_ramp(const uint64_t* offsets, uint64_t n, uint64_t cap, std::vector<Chunk>& out) {
     out.clear();
+    const uint64_t end = offsets[n], lim = kMaxBatchBytes - 64;
+    cap = std::max<uint64_t>(std::min(cap, lim), 1);
+    double size = (double)cap / (1.3 * 1.3 * 1.3);
     uint64_t s = 0;
     while (s < n) {
-        const uint64_t* hi = std::upper_bound(offsets + s + 1, offsets + n + 1, offsets[s] + cap);
-        uint64_t e = (uint64_t)(hi - offsets) - 1;  // last index with offsets[e] <= offsets[s] + cap
+        uint64_t want = (uint64_t)std::min<double>(size, (double)cap);
+        const uint64_t left = end - offsets[s];
+        if (left < want + cap / 4 && left <= lim) want = left;
+        const uint64_t* hi = std::upper_bound(offsets + s + 1, offsets + n + 1, offsets[s] + want);
+        uint64_t e = (uint64_t)(hi - offsets) - 1;  // last index with offsets[e] <= offsets[s] + want
         if (e <= s) e = s + 1;
         if (offsets[e] - offsets[s] > kMaxBatchBytes - 64)
             return fail_kind(SCB_ERR_INTERNAL_STATE, "a single sequence longer than 2 GiB is not supported");
         out.push_back(Chunk{s, e, offsets[s], offsets[e], 0});
         s = e;
+        size *= 1.3;
     }
     return SCB_OK;
 }
@@ -1268,8 +1277,9 @@ static scb_status build_stream_batch(scb_ctx* ctx, Lane& L, const uint8_t* d_seq
     return SCB_OK;
 }
 
-// Default sequence bytes per piece of a host build + stream query (whole sequences).
-constexpr uint64_t kPieceBytes = 768ull << 20;
+// Default largest piece of a host build + stream query (whole sequences; the first pieces are
+// smaller, plan_ramp).
+constexpr uint64_t kPieceBytes = 512ull << 20;
 
 
 // Host build + stream query of a large batch in pieces, each in its own lane: piece p + 1 is
@@ -1284,7 +1294,7 @@ static scb_status build_stream_pieces(scb_ctx* ctx, const uint8_t* seqs, const u
     const uint64_t piece_bytes = ctx->piece_bytes ? ctx->piece_bytes : kPieceBytes;
     if (!ctx->graphs || !probes_fit(ctx) || total < 2 * piece_bytes) return SCB_OK;
     std::vector<Chunk> pieces;
-    SCB_TRY(plan_pieces(offsets, n, piece_bytes, pieces));
+    SCB_TRY(plan_ramp(offsets, n, piece_bytes, pieces));
     if (pieces.size() < 2) return SCB_OK;
     for (const Chunk& c : pieces) {
         const uint64_t b = c.byte1 - c.byte0;
