@@ -129,11 +129,14 @@ struct Chunk {
 // next 1.3x larger, up to cap, so the first copy (which no work overlaps) is short while later
 // copies stay ahead of the work on the pieces before them; a tail under cap / 4 joins the piece
 // before it.  One longer sequence goes alone.
+uint64_t ramp_cap(uint64_t cap) { return std::max<uint64_t>(std::min<uint64_t>(cap, kMaxBatchBytes - 64), 1); }
+double ramp_first(uint64_t cap) { return (double)ramp_cap(cap) / (1.3 * 1.3 * 1.3); }
+
 scb_status plan_ramp(const uint64_t* offsets, uint64_t n, uint64_t cap, std::vector<Chunk>& out) {
     out.clear();
     const uint64_t end = offsets[n], lim = kMaxBatchBytes - 64;
-    cap = std::max<uint64_t>(std::min(cap, lim), 1);
-    double size = (double)cap / (1.3 * 1.3 * 1.3);
+    double size = ramp_first(cap);
+    cap = ramp_cap(cap);
     uint64_t s = 0;
     while (s < n) {
         uint64_t want = (uint64_t)std::min<double>(size, (double)cap);
@@ -1287,12 +1290,46 @@ constexpr uint64_t kPieceBytes = 512ull << 20;
 // its super-k-mer records and probe slots, and after the last insert each piece's query runs on
 // what it kept.  done = false: the batch is not split (small, graphs off, or a strategy other
 // than grouped for some piece), and the caller runs it as one batch.
+// Piece lanes, their upload events and the copy stream, for P pieces.
+static scb_status ensure_pieces(scb_ctx* ctx, size_t P) {
+    while (ctx->piece_lanes.size() < P) ctx->piece_lanes.push_back(std::make_unique<Lane>());
+    while (ctx->piece_events.size() < P) {
+        cudaEvent_t e;
+        SCB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        ctx->piece_events.push_back(e);
+    }
+    if (!ctx->copy_stream) SCB_CUDA(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+    return SCB_OK;
+}
+
+static bool pieces_apply(const scb_ctx* ctx, uint64_t total) {
+    const uint64_t piece_bytes = ctx->piece_bytes ? ctx->piece_bytes : kPieceBytes;
+    return ctx->graphs && probes_fit(ctx) && total >= 2 * piece_bytes;
+}
+
+// Starts the copy of the first piece's bytes (the ramp's first size, which needs no offsets) to
+// the first piece lane, so that it runs while the host validates the offsets.  pre = the bytes
+// in flight on the copy stream (0: none).  Reads only inside [offsets[0], offsets[n]).
+static scb_status preload_first_piece(scb_ctx* ctx, const uint8_t* seqs, const uint64_t* offsets, uint64_t n,
+                                      uint64_t& pre) {
+    pre = 0;
+    if (!seqs || !n || offsets[n] < offsets[0] || !pieces_apply(ctx, offsets[n] - offsets[0])) return SCB_OK;
+    const uint64_t first = (uint64_t)ramp_first(ctx->piece_bytes ? ctx->piece_bytes : kPieceBytes);
+    if (!first || first >= offsets[n] - offsets[0]) return SCB_OK;
+    SCB_TRY(ensure_pieces(ctx, 1));
+    Lane& L = *ctx->piece_lanes[0];
+    SCB_TRY(L.ascii.ensure((first + 31) / 32 * 32 + 64));
+    SCB_CUDA(cudaMemcpyAsync(L.ascii.p, seqs + offsets[0], first, cudaMemcpyHostToDevice, ctx->copy_stream));
+    pre = first;
+    return SCB_OK;
+}
+
 static scb_status build_stream_pieces(scb_ctx* ctx, const uint8_t* seqs, const uint64_t* offsets, uint64_t n,
-                                      uint64_t* kmers, uint64_t* smers, scb_report* rep, bool& done) {
+                                      uint64_t pre, uint64_t* kmers, uint64_t* smers, scb_report* rep, bool& done) {
     done = false;
     const uint64_t total = n ? offsets[n] - offsets[0] : 0;
     const uint64_t piece_bytes = ctx->piece_bytes ? ctx->piece_bytes : kPieceBytes;
-    if (!ctx->graphs || !probes_fit(ctx) || total < 2 * piece_bytes) return SCB_OK;
+    if (!pieces_apply(ctx, total)) return SCB_OK;
     std::vector<Chunk> pieces;
     SCB_TRY(plan_ramp(offsets, n, piece_bytes, pieces));
     if (pieces.size() < 2) return SCB_OK;
@@ -1304,24 +1341,20 @@ static scb_status build_stream_pieces(scb_ctx* ctx, const uint8_t* seqs, const u
         }
     }
     const size_t P = pieces.size();
-    while (ctx->piece_lanes.size() < P) ctx->piece_lanes.push_back(std::make_unique<Lane>());
-    while (ctx->piece_events.size() < P) {
-        cudaEvent_t e;
-        SCB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-        ctx->piece_events.push_back(e);
-    }
-    if (!ctx->copy_stream) SCB_CUDA(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+    SCB_TRY(ensure_pieces(ctx, P));
     Lane& main = ctx->lane;
     SCB_TRY(ensure_lane_work(ctx, main, 0));  // its stream runs the pieces
     cudaStream_t cs = main.stream, xs = ctx->copy_stream;
     // pinned reads are copied asynchronously; pageable ones block the host per copy, which still
-    // overlaps the GPU's work on the pieces already launched
+    // overlaps the GPU's work on the pieces already launched.  The first piece's bytes are already
+    // on their way when it fits the preloaded size (a longer first sequence reallocates the
+    // buffer, after the copy, and copies the piece again).
     auto upload = [&](size_t p) -> scb_status {
         const Chunk& c = pieces[p];
         Lane& L = *ctx->piece_lanes[p];
         const uint64_t ns = c.seq1 - c.seq0, nb = c.byte1 - c.byte0;
         SCB_TRY(ensure_lane(ctx, L, nb, ns));
-        SCB_CUDA(cudaMemcpyAsync(L.ascii.p, seqs + c.byte0, nb, cudaMemcpyHostToDevice, xs));
+        if (p != 0 || nb > pre) SCB_CUDA(cudaMemcpyAsync(L.ascii.p, seqs + c.byte0, nb, cudaMemcpyHostToDevice, xs));
         SCB_CUDA(cudaMemcpyAsync(L.offsets.p, offsets + c.seq0, (ns + 1) * 8, cudaMemcpyHostToDevice, xs));
         SCB_CUDA(cudaEventRecord(ctx->piece_events[p], xs));
         return SCB_OK;
@@ -1401,13 +1434,24 @@ scb_status scb_build_and_stream_query(scb_ctx* ctx, const uint8_t* seqs, const u
     {
         CtxLock lk(ctx);
         if (ctx->frozen) return fail_kind(SCB_ERR_INTERNAL_STATE, "the index is frozen; inserts need a builder");
-        SCB_TRY(check_offsets(offsets, n));
+        if (!offsets) return fail_kind(SCB_ERR_INTERNAL_STATE, "null offsets");
+        // the first piece's bytes copy while the offsets are validated; every return below
+        // waits for that copy, which reads the caller's buffer
+        uint64_t pre = 0;
+        SCB_TRY(preload_first_piece(ctx, seqs, offsets, n, pre));
+        const scb_status vs = check_offsets(offsets, n);
+        if (vs != SCB_OK) {
+            if (pre) cudaStreamSynchronize(ctx->copy_stream);
+            return vs;
+        }
         const uint64_t total = n ? offsets[n] - offsets[0] : 0;
         std::memset(rep, 0, sizeof(*rep));
         if (kmers) *kmers = 0;
         if (smers) *smers = 0;
         bool done = false;
-        SCB_TRY(build_stream_pieces(ctx, seqs, offsets, n, kmers, smers, rep, done));
+        const scb_status ps = build_stream_pieces(ctx, seqs, offsets, n, pre, kmers, smers, rep, done);
+        if (pre && (ps != SCB_OK || !done)) SCB_CUDA(cudaStreamSynchronize(ctx->copy_stream));
+        SCB_TRY(ps);
         if (done) return SCB_OK;
         if (total <= kMaxBatchBytes - 64) {
             // one resident batch: copy once, insert, freeze, query the same staged codes (and,

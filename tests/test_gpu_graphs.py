@@ -205,11 +205,12 @@ def test_build_and_stream_probe_slots_overflow(scb, oracle_mod, graphs):
     ctx.close()
 
 
-@pytest.mark.parametrize("pinned", [False, True])
-def test_host_build_and_stream_in_pieces_matches_oracle(scb, oracle_mod, pinned):
+@pytest.mark.parametrize("pinned,long_first", [(False, False), (True, False), (True, True)])
+def test_host_build_and_stream_in_pieces_matches_oracle(scb, oracle_mod, pinned, long_first):
     """The host build + stream query split into pieces (copy of piece p + 1 overlapping the insert
     of piece p, each piece queried on its kept records after the last insert) gives exactly the
-    oracle's counts, report and table, from pageable or pinned host memory."""
+    oracle's counts, report and table, from pageable or pinned host memory, also when the first
+    sequence is longer than the first piece's bytes copied while the offsets are validated."""
     import torch
 
     from scbf_b200 import _lib, api
@@ -217,7 +218,10 @@ def test_host_build_and_stream_in_pieces_matches_oracle(scb, oracle_mod, pinned)
     L = _lib.load()
     cfg = scb.SuperCountingBloomConfig(k=31, m=21, s=25, n_hashes=4, counter_bits=scb.CounterBits(16),
                                        counter_slots_exponent=22, block_slots_exponent=9, threads=3, queue=17)
-    data, offsets = scb.pack_sequences(_reads(51, 9000, 100, 1200))
+    seqs = _reads(51, 9000, 100, 1200)
+    if long_first:  # 700 kB, above the 0.45 MiB first piece of 1 MiB pieces
+        seqs = _reads(52, 1, 700_000, 700_000) + seqs
+    data, offsets = scb.pack_sequences(seqs)
     o = oracle_mod.OracleFilter(oracle_mod.make_config(31, 21, 25, 4, 16, 22, 9, 3, 17))
     okm, osm = o.insert_batch_arrays(data, offsets)
     oq = o.query_report_arrays(data, offsets)
