@@ -310,6 +310,9 @@ void launch_scan_inplace(uint64_t* data, uint64_t n, uint64_t* scratch, cudaStre
 constexpr int kBack = 32;  // windows evaluated before a tile in stats mode (>= w)
 constexpr int kFwd = 1;    // windows evaluated after a tile (super-k-mer end detection)
 constexpr int kEvalMax = kTileWindows + kBack + kFwd;
+// The cut's tiles: kBack windows before and kFwd after fill kTileWindows evaluated windows exactly,
+// so every window's minimum comes from the four-window strips.
+constexpr int kCutWindows = kTileWindows - kBack - kFwd;
 constexpr int kKeysMax = kEvalMax + 32;
 constexpr int kCodeWordsMax = (kEvalMax + 96 + 16) / 16 + 8;
 constexpr int kBitWordsMax = (kEvalMax + 128 + 32) / 32 + 8;
@@ -322,7 +325,7 @@ struct TileSmem {
     uint32_t valid[kBitWordsMax];
     uint32_t start[kBitWordsMax];
     uint32_t pk[kKeysMax];  // packed m-mer key: (hash >> 16) << 16 | position relative to e0
-    uint16_t poff[kEvalMax];
+    alignas(8) uint16_t poff[kEvalMax];
     uint32_t block[kEvalMax];
     uint16_t ends[kTileWindows];
     // canonical ntHash tables: 3-base chunk contributions (fw, rc) and one-base roll terms
@@ -334,6 +337,7 @@ struct TileSmem {
     uint32_t tile;
     uint64_t seq_lo, seq_hi;
     uint32_t warp_cnt[kTileThreads / 32];
+    uint32_t warp_run[kTileThreads / 32];
 };
 
 
@@ -490,6 +494,8 @@ __global__ void __launch_bounds__(kTileThreads, 8) k_tiles(TileArgs a) {
         n_code_words = 2 * n_bit_words;
         n_tiles = (uint32_t)((n_bytes + kTileWindows - 1) / kTileWindows);
     }
+    constexpr uint32_t kWin = MODE == kModeCut ? (uint32_t)kCutWindows : (uint32_t)kTileWindows;  // tile windows
+    if constexpr (MODE == kModeCut) n_tiles = (uint32_t)((n_bytes + kWin - 1) / kWin);
     fill_nt_tables(sm, g.m);
 
     while (true) {
@@ -497,12 +503,12 @@ __global__ void __launch_bounds__(kTileThreads, 8) k_tiles(TileArgs a) {
         __syncthreads();
         const uint32_t tile = sm.tile;
         if (tile >= n_tiles) break;
-        const uint64_t t0 = (uint64_t)tile * kTileWindows;
+        const uint64_t t0 = (uint64_t)tile * kWin;
         const uint32_t back = (MODE == kModeStats || MODE == kModeCut)
                                   ? (uint32_t)(t0 < (uint64_t)kBack ? t0 : (uint64_t)kBack)
                                   : 0u;
         const uint64_t e0 = t0 - back;
-        const uint32_t n_eval = back + kTileWindows + kFwd;
+        const uint32_t n_eval = MODE == kModeCut ? (uint32_t)kTileWindows : back + kTileWindows + kFwd;
         const uint32_t n_keys = n_eval + g.w - 1;
 
         // stage codes and bitmaps of the tile
@@ -689,44 +695,72 @@ __global__ void __launch_bounds__(kTileThreads, 8) k_tiles(TileArgs a) {
             }
         } else if constexpr (MODE == kModeCut) {
             // one record per super-k-mer, emitted at its last window: (block, first window, windows).
-            constexpr uint32_t kPer = kTileWindows / kTileThreads;
+            // Thread t looks at evaluated windows 4t .. 4t+3 (its strip); the tile's own windows
+            // are [back, back + kCutWindows).  A window starts a super-k-mer when its minimizer
+            // position differs from the window before, and ends one when it differs from the
+            // window after.  A block-wide running maximum of start positions gives each end its
+            // first window (a super-k-mer spans at most w <= 32 = kBack windows, so every one
+            // that ends in the tile starts inside the evaluated range).
             const uint32_t lane = tid & 31, wid = tid >> 5;
-            uint32_t mine = 0;  // ends among this thread's windows back + tid*kPer .. + kPer - 1
-            for (uint32_t r = 0; r < kPer; r++) {
-                const uint32_t i = back + tid * kPer + r;
-                const uint16_t po = sm.poff[i];
-                c_win += po != kNoWindow;
-                mine += (po != kNoWindow && sm.poff[i + 1] != po) ? 1u : 0u;
+            const uint32_t i0 = 4 * tid;
+            const uint2 raw = *reinterpret_cast<const uint2*>(sm.poff + i0);
+            const uint32_t p[4] = {raw.x & 0xFFFFu, raw.x >> 16, raw.y & 0xFFFFu, raw.y >> 16};
+            const uint32_t pv = tid ? (uint32_t)sm.poff[i0 - 1] : (uint32_t)kNoWindow;
+            const uint32_t pn = sm.poff[i0 + 4];  // index kTileWindows: never a tile window's successor
+            const uint32_t lo = back, hi = back + (uint32_t)kCutWindows;
+            uint32_t mine = 0, run = 0, endmask = 0;
+            uint32_t rs[4];  // 1 + the latest start in this strip up to each window (0: none yet)
+#pragma unroll
+            for (uint32_t j = 0; j < 4; j++) {
+                const uint32_t i = i0 + j;
+                const uint32_t before = j ? p[j - 1] : pv, after = j < 3 ? p[j + 1] : pn;
+                const bool ok = p[j] != kNoWindow;
+                if (ok && before != p[j]) run = i + 1;
+                rs[j] = run;
+                const bool in = i >= lo && i < hi;
+                c_win += (ok && in) ? 1u : 0u;
+                if (ok && in && after != p[j]) {
+                    endmask |= 1u << j;
+                    mine++;
+                }
             }
-            uint32_t incl = mine;
+            uint32_t incl = mine, rmax = run;
             for (int off = 1; off < 32; off <<= 1) {
                 const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, off);
-                if ((int)lane >= off) incl += y;
+                const uint32_t z = __shfl_up_sync(0xFFFFFFFFu, rmax, off);
+                if ((int)lane >= off) {
+                    incl += y;
+                    rmax = max(rmax, z);
+                }
             }
-            if (lane == 31) sm.warp_cnt[wid] = incl;
+            uint32_t rprev = __shfl_up_sync(0xFFFFFFFFu, rmax, 1);
+            if (lane == 0) rprev = 0;
+            if (lane == 31) {
+                sm.warp_cnt[wid] = incl;
+                sm.warp_run[wid] = rmax;
+            }
             __syncthreads();
             uint32_t before = incl - mine, tile_total = 0;
             for (uint32_t x = 0; x < kTileThreads / 32; x++) {
                 const uint32_t c = sm.warp_cnt[x];
                 before += x < wid ? c : 0u;
                 tile_total += c;
+                if (x < wid) rprev = max(rprev, sm.warp_run[x]);
             }
-            // compact the tile's end windows, in window order, so the per-record work below runs
-            // on full warps
-            for (uint32_t r = 0; r < kPer; r++) {
-                const uint32_t i = back + tid * kPer + r;
-                const uint16_t po = sm.poff[i];
-                if (po != kNoWindow && sm.poff[i + 1] != po) sm.ends[before++] = (uint16_t)i;
+            // compact the tile's ends (window | first window << 16, in window order, in the block
+            // array the cut does not otherwise use) so the per-record work below runs on full warps
+#pragma unroll
+            for (uint32_t j = 0; j < 4; j++) {
+                if ((endmask >> j) & 1u) sm.block[before++] = (i0 + j) | ((max(rprev, rs[j]) - 1u) << 16);
             }
             __syncthreads();
             // each record takes the next slot of its bucket's region; past the region it goes to
             // the overflow list (sorted into place by the bucketing step)
             const uint32_t local_mask = (1u << a.bucket_shift) - 1u;
             for (uint32_t e = tid; e < tile_total; e += blockDim.x) {
-                const uint32_t i = sm.ends[e];
+                const uint32_t v = sm.block[e];
+                const uint32_t i = v & 0xFFFFu, st = v >> 16;
                 const uint16_t po = sm.poff[i];
-                uint32_t st = i;
-                while (st > 0 && sm.poff[st - 1] == po) st--;
                 const uint32_t nwin = i - st + 1;
                 c_sk++;
                 c_smer += nwin + ks;
