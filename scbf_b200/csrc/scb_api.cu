@@ -347,6 +347,8 @@ scb_status grouped_buffers(Lane& L, const GroupedSizes& z) {
     SCB_TRY(L.rec_key.ensure(z.cap * 4));
     SCB_TRY(L.rec_val.ensure(z.cap * 8));
     SCB_TRY(L.rec_sorted.ensure((z.region() + z.cap) * 8));
+    SCB_TRY(L.rec_bases.ensure(z.cap * 16));
+    SCB_TRY(L.rec_sbases.ensure((z.region() + z.cap) * 16));
     SCB_TRY(L.items.ensure(z.max_items * 16));
     return SCB_OK;
 }
@@ -362,6 +364,8 @@ scb_status launch_cut(scb_ctx* ctx, Lane& L, TileArgs& a, const GroupedSizes& z,
     a.bucket_hist = L.bhist.as<unsigned long long>();
     a.bucket_shift = z.shift;
     a.sorted = L.rec_sorted.as<unsigned long long>();
+    a.sbases = L.rec_sbases.as<uint4>();
+    a.rec_bases = L.rec_bases.as<uint4>();
     a.bucket_cap = z.bucket_cap;
     if (a.n_tiles == 0) return SCB_OK;
     SCB_CUDA(cudaMemsetAsync(L.tiles.p, 0, 4, st));
@@ -384,9 +388,9 @@ scb_status launch_bucketing(scb_ctx* ctx, Lane& L, const GroupedSizes& z, cudaSt
     launch_item_write(counts, z.bucket_cap, L.icount.as<uint64_t>(), ovf, z.region(), z.n_buckets,
                       L.items.as<uint4>(), st);
     // the overflow cursors start at the overflow offsets, which item_write has read
-    launch_scatter(L.rec_key.as<uint32_t>(), L.rec_val.as<unsigned long long>(),
+    launch_scatter(L.rec_key.as<uint32_t>(), L.rec_val.as<unsigned long long>(), L.rec_bases.as<uint4>(),
                    L.rec_count.as<unsigned long long>(), z.cap, z.shift, L.bcursor.as<unsigned long long>(),
-                   z.region(), L.rec_sorted.as<unsigned long long>(), st);
+                   z.region(), L.rec_sorted.as<unsigned long long>(), L.rec_sbases.as<uint4>(), st);
     SCB_CUDA(cudaGetLastError());
     return SCB_OK;
 }
@@ -400,6 +404,7 @@ GroupArgs group_args(const scb_ctx* ctx, const Lane& L, const TileArgs& a, const
     ga.table = ctx->table;
     ga.status = ctx->status;
     ga.recs = L.rec_sorted.as<unsigned long long>();
+    ga.sbases = L.rec_sbases.as<uint4>();
     ga.items = L.items.as<uint4>();
     ga.n_items = reinterpret_cast<const unsigned long long*>(L.icount.as<uint64_t>() + z.n_buckets);
     ga.work_counter = L.tiles.as<unsigned int>() + 1;
@@ -598,7 +603,8 @@ constexpr size_t kMaxGraphsPerLane = 8;
 
 uint64_t lane_signature(const scb_ctx* ctx, const Lane& L) {
     const void* ptrs[] = {L.codes.p, L.valid.p, L.seqstart.p, L.cnt.p, L.cnt2.p, L.tiles.p, L.params.p,
-                          L.rec_key.p, L.rec_val.p, L.rec_sorted.p, L.bhist.p, L.bcursor.p, L.icount.p,
+                          L.rec_key.p, L.rec_val.p, L.rec_sorted.p, L.rec_bases.p, L.rec_sbases.p, L.bhist.p,
+                          L.bcursor.p, L.icount.p,
                           L.items.p, L.gscan.p, L.rec_count.p, L.probes.p, L.item_base.p, ctx->table, ctx->status};
     uint64_t h = 0x243F6A8885A308D3ull;
     for (const void* q : ptrs) h = (h ^ (uint64_t)(uintptr_t)q) * 0x100000001B3ull + 0x9E3779B97F4A7C15ull;

@@ -161,6 +161,7 @@ struct Lane {
     DevBuf ascii, offsets, codes, valid, seqstart, woff, scan, wblock, wend, cnt, cnt2, tiles, params;
     // grouped pipeline: records, bucket offsets / cursors, work items
     DevBuf rec_key, rec_val, rec_sorted, bhist, bcursor, icount, items, gscan, rec_count;
+    DevBuf rec_bases, rec_sbases;  // 16-byte base entries of the overflow and the sorted records
     // probe slots kept from a grouped insert for the query of the same records (build + stream)
     DevBuf probes, item_base;
     bool want_probes = false;

@@ -767,16 +767,23 @@ __global__ void __launch_bounds__(kTileThreads, 8) k_tiles(TileArgs a) {
                 const uint32_t block = minimizer_block(sm.codes, e0 + po - cb, g);
                 const unsigned long long val =
                     (unsigned long long)(e0 + st) | ((unsigned long long)nwin << kRecWindowsShift);
+                // the super-k-mer's bases (64 from its first one) travel with the record, so the
+                // apply reads them in slot order instead of gathering them from the batch's codes
+                const uint32_t b0 = (uint32_t)(e0 + st - cb);
+                const uint64_t lo = codes64(sm.codes, b0), hi = codes64(sm.codes, b0 + 32u);
+                const uint4 bases4 = make_uint4((uint32_t)lo, (uint32_t)(lo >> 32), (uint32_t)hi, (uint32_t)(hi >> 32));
                 const uint32_t bucket = block >> a.bucket_shift;
                 const unsigned long long slot = atomicAdd(a.bucket_hist + bucket, 1ull);
                 if (slot < a.bucket_cap) {
-                    a.sorted[(uint64_t)bucket * a.bucket_cap + slot] =
-                        val | ((unsigned long long)(block & local_mask) << kRecLocalShift);
+                    const uint64_t at = (uint64_t)bucket * a.bucket_cap + slot;
+                    a.sorted[at] = val | ((unsigned long long)(block & local_mask) << kRecLocalShift);
+                    a.sbases[at] = bases4;
                 } else {
                     const unsigned long long o = atomicAdd(a.rec_count, 1ull);
                     if (o < a.rec_cap) {
                         a.rec_key[o] = block;
                         a.rec_val[o] = val;
+                        a.rec_bases[o] = bases4;
                     }
                 }
             }
@@ -1019,9 +1026,9 @@ void launch_counter_hist(const void* table, uint64_t slots, int bits, unsigned l
 // Overflow records (those past their bucket's region) into bucket order after the regions:
 // position = base + the bucket's overflow offset + its running count.
 __global__ void k_scatter(const uint32_t* __restrict__ key, const unsigned long long* __restrict__ val,
-                          const unsigned long long* __restrict__ count, uint64_t cap, uint32_t shift,
-                          unsigned long long* __restrict__ cursor, uint64_t base,
-                          unsigned long long* __restrict__ sorted) {
+                          const uint4* __restrict__ vbases, const unsigned long long* __restrict__ count,
+                          uint64_t cap, uint32_t shift, unsigned long long* __restrict__ cursor, uint64_t base,
+                          unsigned long long* __restrict__ sorted, uint4* __restrict__ sbases) {
     const uint64_t n = *count;
     if (n > cap) return;  // the overflow list ran out of room: the host redoes the batch
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
@@ -1031,6 +1038,7 @@ __global__ void k_scatter(const uint32_t* __restrict__ key, const unsigned long 
         const uint32_t block = key[i];
         const unsigned long long pos = base + atomicAdd(cursor + (block >> shift), 1ull);
         sorted[pos] = v | ((unsigned long long)(block & local_mask) << kRecLocalShift);
+        sbases[pos] = vbases[i];
     }
 }
 
@@ -1162,10 +1170,10 @@ struct ApplyLayout {
 
 // s-mers (and windows) of one staged chunk of records; a record has at most 31 + 31
 constexpr uint32_t kSmerBudget = 4096;
-// 2-bit code words staged per record: its <= 61 bases (at most w = k - m + 1 windows of odd
-// k <= 31 bases) start at most 15 bases after a 16-base boundary, so they end in word 4.
-// codes64 may read up to two words further; those bits lie past the s-mer and are masked off.
-constexpr uint32_t kRecBaseWords = 5;
+// 2-bit code words staged per record: its record bases, whose first base is the first window's,
+// hold its <= w + k - 1 <= 63 bases.  codes64 may read up to two words further (into the next
+// record's words or the spare words); those bits lie past the s-mer and are masked off.
+constexpr uint32_t kRecBaseWords = 4;
 // probe-slot loads a query thread keeps in flight
 constexpr uint32_t kProbeBatch = 4;
 
@@ -1317,14 +1325,13 @@ __device__ __forceinline__ void apply_body(const GroupArgs& a, uint32_t bs_log2,
             chunk_prefix(rv, nrec, ks, spre, wpre, warp_tot);
             // the leading records whose s-mers fit the chunk's budget (at least one)
             const uint32_t nuse = (uint32_t)__syncthreads_count(tid < nrec && spre[tid + 1] <= kSmerBudget);
-            // stage the records' bases, kRecBaseWords consecutive threads per record (one sector
-            // read, conflict-free shared stores), and their reverse complements (a query with the
-            // insert's probe slots needs no bases)
-            for (uint32_t x = tid; x < (have_probes || LEAN ? 0u : nuse * kRecBaseWords); x += blockDim.x) {
-                const uint32_t r = x / kRecBaseWords, j = x % kRecBaseWords;
-                const uint32_t cw = __ldg(a.codes + ((uint32_t)rv[r] >> 4) + j);
-                bases[x] = cw;
-                rbases[r * kRecBaseWords + (kRecBaseWords - 1 - j)] = revcomp16(cw);
+            // stage the records' bases (one 16-byte entry per record, read in slot order) and
+            // their reverse complements (a query with the insert's probe slots needs no bases)
+            for (uint32_t r = tid; r < (have_probes || LEAN ? 0u : nuse); r += blockDim.x) {
+                const uint4 b = __ldcs(a.sbases + first + c0 + r);
+                reinterpret_cast<uint4*>(bases)[r] = b;
+                reinterpret_cast<uint4*>(rbases)[r] = make_uint4(revcomp16(b.w), revcomp16(b.z), revcomp16(b.y),
+                                                                 revcomp16(b.x));
             }
             if (tid < nuse) {  // record index of its s-mers (not needed with kept slots) / windows
                 const uint32_t s0 = spre[tid], s1 = have_probes ? s0 : spre[tid + 1];
@@ -1378,7 +1385,7 @@ __device__ __forceinline__ void apply_body(const GroupArgs& a, uint32_t bs_log2,
                 const unsigned long long v = rv[r];
                 const uint32_t lb = (uint32_t)(v >> kRecLocalShift);
                 const uint32_t start = (uint32_t)v;
-                const uint32_t rel = (start & 15u) + (f - spre[r]);  // base offset in the staged words
+                const uint32_t rel = f - spre[r];  // base offset in the staged words
                 // forward s-mer from the staged words; its reverse complement from the mirrored
                 // words: base t of it is the complement of forward base rel + s - 1 - t, which
                 // sits at position 16 * kRecBaseWords - rel - s + t of the mirrored stream (bits
@@ -1594,12 +1601,13 @@ void launch_apply(int mode, const GroupArgs& a, int bs_log2, uint32_t bucket_blo
     }
 }
 
-void launch_scatter(const uint32_t* rec_key, const unsigned long long* rec_val, const unsigned long long* rec_count,
-                    uint64_t rec_cap, uint32_t bucket_shift, unsigned long long* cursor, uint64_t base,
-                    unsigned long long* sorted, cudaStream_t st) {
+void launch_scatter(const uint32_t* rec_key, const unsigned long long* rec_val, const uint4* rec_bases,
+                    const unsigned long long* rec_count, uint64_t rec_cap, uint32_t bucket_shift,
+                    unsigned long long* cursor, uint64_t base, unsigned long long* sorted, uint4* sbases,
+                    cudaStream_t st) {
     const uint64_t blocks = (rec_cap + 255) / 256;
     k_scatter<<<(unsigned)(blocks < 4096 ? (blocks ? blocks : 1) : 4096), 256, 0, st>>>(
-        rec_key, rec_val, rec_count, rec_cap, bucket_shift, cursor, base, sorted);
+        rec_key, rec_val, rec_bases, rec_count, rec_cap, bucket_shift, cursor, base, sorted, sbases);
     note_launch();
 }
 

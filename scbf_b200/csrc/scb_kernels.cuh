@@ -40,6 +40,9 @@ struct BatchParams {
 // Grouped pipeline: super-k-mer records bucketed by counter block.
 // Overflow record: key = block id, val = first window position | windows << 32.
 // Sorted record:   val = first window position | windows << 32 | block-in-bucket << 38.
+// Record bases:    the super-k-mer's 2-bit codes from its first window's first base, 64 bases
+//                  (at most w + k - 1 <= 63 are its own) in one 16-byte entry per record, slot for
+//                  slot beside the overflow list and the sorted records.
 constexpr uint32_t kRecWindowsShift = 32;
 constexpr uint32_t kRecLocalShift = 38;
 constexpr uint32_t kItemRecords = 4096;    // records per work item (heavier buckets are split)
@@ -55,6 +58,7 @@ struct GroupArgs {
     uint32_t* status;
     unsigned long long* cnt;
     const unsigned long long* recs;  // sorted records
+    const uint4* sbases;             // their bases, slot for slot
     const uint4* items;              // {bucket, first record, records, exclusive}
     const unsigned long long* n_items;
     unsigned int* work_counter;
@@ -136,6 +140,8 @@ struct TileArgs {
     uint32_t pad3_;
     unsigned long long* sorted;
     uint64_t bucket_cap;
+    uint4* sbases;     // bases of the records in sorted, slot for slot
+    uint4* rec_bases;  // bases of the overflow records
     // when set, n_bytes / n_seqs / offsets come from here at run time (graph replays) and the
     // fields above give the capacity of the batch's shape class
     const BatchParams* dyn;
@@ -167,9 +173,10 @@ void launch_counter_hist(const void* table, uint64_t slots, int bits, unsigned l
                          unsigned long long* ovf, uint64_t ovf_cap, unsigned long long* ovf_count, cudaStream_t st);
 void launch_fill_u32(uint32_t* p, uint32_t v, uint64_t n, cudaStream_t st);
 // grouped pipeline
-void launch_scatter(const uint32_t* rec_key, const unsigned long long* rec_val, const unsigned long long* rec_count,
-                    uint64_t rec_cap, uint32_t bucket_shift, unsigned long long* cursor, uint64_t base,
-                    unsigned long long* sorted, cudaStream_t st);
+void launch_scatter(const uint32_t* rec_key, const unsigned long long* rec_val, const uint4* rec_bases,
+                    const unsigned long long* rec_count, uint64_t rec_cap, uint32_t bucket_shift,
+                    unsigned long long* cursor, uint64_t base, unsigned long long* sorted, uint4* sbases,
+                    cudaStream_t st);
 void launch_item_counts(const unsigned long long* counts, uint64_t n_buckets, uint64_t bucket_cap, uint64_t* item_count,
                         uint64_t* ovf_count, const unsigned long long* rec_count, uint64_t rec_cap, cudaStream_t st);
 void launch_item_write(const unsigned long long* counts, uint64_t bucket_cap, const uint64_t* item_off,
