@@ -777,7 +777,7 @@ __global__ void __launch_bounds__(kTileThreads, 8) k_tiles(TileArgs a) {
                 if (slot < a.bucket_cap) {
                     const uint64_t at = (uint64_t)bucket * a.bucket_cap + slot;
                     a.sorted[at] = val | ((unsigned long long)(block & local_mask) << kRecLocalShift);
-                    a.sbases[at] = bases4;
+                    __stcs(a.sbases + at, bases4);  // read once, by the apply
                 } else {
                     const unsigned long long o = atomicAdd(a.rec_count, 1ull);
                     if (o < a.rec_cap) {
