@@ -230,8 +230,9 @@ scb_status scb_graph_stats(const scb_ctx* ctx, uint64_t* captures, uint64_t* rep
 
 /* Host scb_build_and_stream_query in pieces (no counterpart in the reference; the reference's
  * parser thread feeds its workers the same way, src/api.rs:621-674).  A batch of at least two
- * pieces is split into pieces of whole sequences of at most piece_bytes (0: 512 MiB), the first
- * piece_bytes / 2.2 and each next 1.3x larger, so the first copy, which nothing overlaps, is
+ * pieces is split into pieces of whole sequences of at most piece_bytes (0: 512 MiB; raised so
+ * that a batch has at most about 32 pieces), the first piece_bytes / 2.2 and each next 1.3x
+ * larger, so the first copy, which nothing overlaps, is
  * short; piece p + 1 is copied to the device while piece p is inserted, every piece keeps its super-k-mer records
  * for its query after the last insert, so the copy overlaps the work.  Applies with graphs on and
  * the grouped strategy; results are identical to one batch. */

@@ -1291,11 +1291,6 @@ static scb_status build_stream_batch(scb_ctx* ctx, Lane& L, const uint8_t* d_seq
 constexpr uint64_t kPieceBytes = 512ull << 20;
 
 
-// Host build + stream query of a large batch in pieces, each in its own lane: piece p + 1 is
-// copied to the device on the copy stream while piece p's insert graph runs, every piece keeps
-// its super-k-mer records and probe slots, and after the last insert each piece's query runs on
-// what it kept.  done = false: the batch is not split (small, graphs off, or a strategy other
-// than grouped for some piece), and the caller runs it as one batch.
 // Piece lanes, their upload events and the copy stream, for P pieces.
 static scb_status ensure_pieces(scb_ctx* ctx, size_t P) {
     while (ctx->piece_lanes.size() < P) ctx->piece_lanes.push_back(std::make_unique<Lane>());
@@ -1308,9 +1303,16 @@ static scb_status ensure_pieces(scb_ctx* ctx, size_t P) {
     return SCB_OK;
 }
 
+// Largest piece of a batch of `total` bytes: the setting (0: kPieceBytes), raised so that a batch
+// has at most about kMaxPieces pieces (each piece has its own lane of device buffers).
+constexpr uint64_t kMaxPieces = 32;
+static uint64_t piece_bytes_for(const scb_ctx* ctx, uint64_t total) {
+    const uint64_t pb = ctx->piece_bytes ? ctx->piece_bytes : kPieceBytes;
+    return std::max<uint64_t>(pb, (total + kMaxPieces - 1) / kMaxPieces);
+}
+
 static bool pieces_apply(const scb_ctx* ctx, uint64_t total) {
-    const uint64_t piece_bytes = ctx->piece_bytes ? ctx->piece_bytes : kPieceBytes;
-    return ctx->graphs && probes_fit(ctx) && total >= 2 * piece_bytes;
+    return ctx->graphs && probes_fit(ctx) && total / 2 >= piece_bytes_for(ctx, total);
 }
 
 // Starts the copy of the first piece's bytes (the ramp's first size, which needs no offsets) to
@@ -1320,7 +1322,7 @@ static scb_status preload_first_piece(scb_ctx* ctx, const uint8_t* seqs, const u
                                       uint64_t& pre) {
     pre = 0;
     if (!seqs || !n || offsets[n] < offsets[0] || !pieces_apply(ctx, offsets[n] - offsets[0])) return SCB_OK;
-    const uint64_t first = (uint64_t)ramp_first(ctx->piece_bytes ? ctx->piece_bytes : kPieceBytes);
+    const uint64_t first = (uint64_t)ramp_first(piece_bytes_for(ctx, offsets[n] - offsets[0]));
     if (!first || first >= offsets[n] - offsets[0]) return SCB_OK;
     SCB_TRY(ensure_pieces(ctx, 1));
     Lane& L = *ctx->piece_lanes[0];
@@ -1330,12 +1332,18 @@ static scb_status preload_first_piece(scb_ctx* ctx, const uint8_t* seqs, const u
     return SCB_OK;
 }
 
+// Host build + stream query of a large batch in pieces, each in its own lane: piece p + 1 is
+// copied to the device on the copy stream while piece p's insert graph runs, every piece keeps
+// its super-k-mer records and probe slots, and after the last insert each piece's query runs on
+// what it kept.  done = false: the batch is not split (small, graphs off, or a strategy other
+// than grouped for some piece), and the caller runs it as one batch.
+// pre = bytes of the first piece already being copied to the first piece lane (preload_first_piece).
 static scb_status build_stream_pieces(scb_ctx* ctx, const uint8_t* seqs, const uint64_t* offsets, uint64_t n,
                                       uint64_t pre, uint64_t* kmers, uint64_t* smers, scb_report* rep, bool& done) {
     done = false;
     const uint64_t total = n ? offsets[n] - offsets[0] : 0;
-    const uint64_t piece_bytes = ctx->piece_bytes ? ctx->piece_bytes : kPieceBytes;
     if (!pieces_apply(ctx, total)) return SCB_OK;
+    const uint64_t piece_bytes = piece_bytes_for(ctx, total);
     std::vector<Chunk> pieces;
     SCB_TRY(plan_ramp(offsets, n, piece_bytes, pieces));
     if (pieces.size() < 2) return SCB_OK;
