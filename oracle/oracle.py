@@ -12,6 +12,7 @@ restated from their published descriptions -- parity unpinned for those parts.
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 import subprocess
 from dataclasses import dataclass
@@ -339,3 +340,92 @@ def sector_stats(cfg: OraConfig, data, offsets) -> tuple[int, int, int]:
     lib().ora_batch_sector_stats(C.byref(cfg), _u8(data), _u64(offsets), len(offsets) - 1,
                                  C.byref(a), C.byref(b), C.byref(c))
     return a.value, b.value, c.value
+
+
+# ---------------------------------------------------------------------------------------
+# Filter-only spectrum (src/api.rs:337-385, 933-1033): host f64 arithmetic over a counter
+# histogram, restated step for step (plain loops, sums left to right) so that every rounding is
+# the reference's.  The checker of scbf_b200.api's vectorised form.
+# ---------------------------------------------------------------------------------------
+def rust_round_u64(x: float) -> int:
+    """`x.round() as u64`: nearest integer with halves away from zero; NaN and negatives give 0,
+    values past u64 saturate."""
+    if not x > 0.0:
+        return 0
+    r = math.floor(x)
+    if x - r >= 0.5:
+        r += 1
+    return min(int(r), (1 << 64) - 1)
+
+
+def filter_only_deconvolved_counts(counter_histogram, n_hashes: int, max_abundance: int) -> list[float]:
+    """src/api.rs:958-1001 (deconvolved_counts): k-mer counts per abundance 1..=max_abundance from
+    the logarithm of the counters' generating function (compound Poisson)."""
+    if max_abundance == 0:
+        return []
+    total = 0
+    for _, counters in counter_histogram:
+        total += counters
+    if total == 0:
+        return [0.0] * max_abundance
+    prob = [0.0] * (max_abundance + 1)
+    for abundance, counters in counter_histogram:
+        if abundance <= max_abundance:
+            prob[abundance] += float(counters) / float(total)
+    p0 = prob[0]
+    if p0 <= 0.0:
+        return []
+    norm = [0.0] * (max_abundance + 1)
+    norm[0] = 1.0
+    for a in range(1, max_abundance + 1):
+        norm[a] = prob[a] / p0
+    logc = [0.0] * (max_abundance + 1)
+    for a in range(1, max_abundance + 1):
+        coef = float(a) * norm[a]
+        for p in range(1, a):
+            coef -= float(p) * logc[p] * norm[a - p]
+        logc[a] = coef / float(a)
+    h = float(max(n_hashes, 1))
+    out = []
+    for a in range(1, max_abundance + 1):
+        v = float(total) * logc[a] / h
+        out.append(v if v > 0.0 else 0.0)  # f64::max(v, 0.0), NaN -> 0
+    return out
+
+
+def _sum_left(values) -> float:
+    t = 0.0
+    for v in values:
+        t += v
+    return t
+
+
+def filter_only_scaled_positive(counter_histogram, max_abundance: int, kmer_count_hint: int) -> list[tuple[int, int]]:
+    """src/api.rs:1003-1022 (scaled_positive_counter_histogram)."""
+    positive = 0
+    for abundance, counters in counter_histogram:
+        if abundance > 0:
+            positive += counters
+    positive_f = float(max(positive, 1))
+    by_value = {}
+    for abundance, counters in counter_histogram:
+        by_value[abundance] = counters
+    return [(a, rust_round_u64(float(kmer_count_hint) * float(by_value.get(a, 0)) / positive_f))
+            for a in range(1, max_abundance + 1)]
+
+
+def filter_only_spectrum(counter_histogram, n_hashes: int, max_abundance: int,
+                         kmer_count_hint: int) -> list[tuple[int, int]]:
+    """src/api.rs:933-956 (estimate_filter_only_spectrum_from_counter_histogram)."""
+    dec = filter_only_deconvolved_counts(counter_histogram, n_hashes, max_abundance)
+    total = _sum_left(dec)
+    if total <= 0.0:
+        return filter_only_scaled_positive(counter_histogram, max_abundance, kmer_count_hint)
+    scale = float(kmer_count_hint) / total
+    return [(a, rust_round_u64(dec[a - 1] * scale)) for a in range(1, max_abundance + 1)]
+
+
+def filter_only_count_hint(counter_histogram, n_hashes: int, max_abundance: int = 255) -> int:
+    """src/api.rs:375-385 (filter_only_count_hint_from_counter_histogram)."""
+    s = _sum_left(filter_only_deconvolved_counts(counter_histogram, n_hashes, max_abundance))
+    return max(rust_round_u64(s), 1)

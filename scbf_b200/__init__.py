@@ -10,6 +10,7 @@ from .api import (  # noqa: F401
     ChannelClosed,
     CounterBits,
     FastxOpen,
+    FilterOnlySpectrumEstimate,
     InternalState,
     InvalidConfig,
     InvalidIndexFormat,

@@ -12,6 +12,7 @@ from __future__ import annotations
 import ctypes as C
 import enum
 import gzip
+import math
 import os
 import time
 from dataclasses import dataclass, field
@@ -203,6 +204,85 @@ class StreamEstimateStats:
 @dataclass
 class StreamEstimateReport:
     stats: StreamEstimateStats
+
+
+@dataclass
+class FilterOnlySpectrumEstimate:
+    """src/api.rs:95-99: rows are (abundance, estimated k-mers) for abundance 1..=max_abundance."""
+    method: str
+    kmer_count_hint: int
+    rows: list
+
+
+# ---------------------------------------------------------------------------------------
+# Filter-only spectrum (src/api.rs:337-385, 933-1033): host f64 arithmetic over the counter
+# histogram the GPU computes.  The k-mer counts per abundance are the coefficients of the
+# logarithm of the counters' generating function (a compound Poisson deconvolution); every
+# product, quotient and sum is taken in the reference's order (sums left to right), so the rows
+# are the reference's to the last bit.
+# ---------------------------------------------------------------------------------------
+_FILTER_ONLY_METHOD = "compound_poisson_counter_deconvolution"
+
+
+def _round_u64(x: float) -> int:
+    """Rust `x.round() as u64`: halves away from zero; NaN and negatives give 0."""
+    if not x > 0.0:
+        return 0
+    r = math.floor(x)
+    if x - r >= 0.5:
+        r += 1
+    return min(int(r), (1 << 64) - 1)
+
+
+def _sum_f64(values: np.ndarray) -> float:
+    """Left-to-right f64 sum (Rust's Iterator::sum; numpy's sum and Python's sum round differently)."""
+    return float(np.add.accumulate(values)[-1]) if len(values) else 0.0
+
+
+def _deconvolved_counts(counter_histogram, n_hashes: int, max_abundance: int) -> np.ndarray:
+    """src/api.rs:958-1001."""
+    if max_abundance == 0:
+        return np.zeros(0)
+    total = sum(int(c) for _, c in counter_histogram)
+    if total == 0:
+        return np.zeros(max_abundance)
+    prob = np.zeros(max_abundance + 1)
+    for abundance, counters in counter_histogram:
+        if abundance <= max_abundance:
+            prob[abundance] += float(counters) / float(total)
+    p0 = float(prob[0])
+    if p0 <= 0.0:
+        return np.zeros(0)
+    norm = prob / p0
+    norm[0] = 1.0
+    idx = np.arange(max_abundance + 1, dtype=np.float64)
+    logc = np.zeros(max_abundance + 1)
+    seq = np.empty(max_abundance + 1)
+    for a in range(1, max_abundance + 1):
+        # a * norm[a] - sum over p = 1 .. a-1 of (p * logc[p]) * norm[a - p], subtracted in order
+        seq[0] = idx[a] * norm[a]
+        seq[1:a] = (idx[1:a] * logc[1:a]) * norm[a - 1:0:-1]
+        logc[a] = float(np.subtract.accumulate(seq[:a])[-1]) / idx[a]
+    v = (float(total) * logc[1:]) / float(max(n_hashes, 1))
+    return np.where(v > 0.0, v, 0.0)
+
+
+def _scaled_positive_counter_histogram(counter_histogram, max_abundance: int, kmer_count_hint: int) -> list:
+    """src/api.rs:1003-1022: the positive counters' histogram scaled to the hint."""
+    positive = float(max(sum(int(c) for a, c in counter_histogram if a > 0), 1))
+    by_value = {int(a): int(c) for a, c in counter_histogram}
+    return [(a, _round_u64(float(kmer_count_hint) * float(by_value.get(a, 0)) / positive))
+            for a in range(1, max_abundance + 1)]
+
+
+def _filter_only_rows(counter_histogram, n_hashes: int, max_abundance: int, kmer_count_hint: int) -> list:
+    """src/api.rs:933-956."""
+    dec = _deconvolved_counts(counter_histogram, n_hashes, max_abundance)
+    total = _sum_f64(dec)
+    if total <= 0.0:
+        return _scaled_positive_counter_histogram(counter_histogram, max_abundance, kmer_count_hint)
+    scale = float(kmer_count_hint) / total
+    return [(a, _round_u64(float(dec[a - 1]) * scale)) for a in range(1, max_abundance + 1)]
 
 
 # ---------------------------------------------------------------------------------------
@@ -535,6 +615,26 @@ class SuperCountingBloomIndex:
         cnts = np.zeros(max(rows.value, 1), np.uint64)
         _check(L.scb_counter_histogram(self._ctx.h, _ptr(vals), _ptr(cnts), rows.value, C.byref(rows)))
         return list(zip(vals[: rows.value].tolist(), cnts[: rows.value].tolist()))
+
+    def estimate_filter_only_spectrum(self, max_abundance: int, kmer_count_hint: int) -> FilterOnlySpectrumEstimate:
+        """src/api.rs:337-348: the k-mer spectrum estimated from the counters alone (no reads)."""
+        return self.estimate_filter_only_spectrum_from_counter_histogram(self.counter_histogram(), max_abundance,
+                                                                         kmer_count_hint)
+
+    def estimate_filter_only_spectrum_from_counter_histogram(self, counter_histogram, max_abundance: int,
+                                                             kmer_count_hint: int) -> FilterOnlySpectrumEstimate:
+        """src/api.rs:350-368."""
+        rows = _filter_only_rows(counter_histogram, int(self._cfg.n_hashes), int(max_abundance), int(kmer_count_hint))
+        return FilterOnlySpectrumEstimate(method=_FILTER_ONLY_METHOD, kmer_count_hint=int(kmer_count_hint), rows=rows)
+
+    def filter_only_count_hint(self) -> int:
+        """src/api.rs:370-373: the deconvolved k-mer total (abundances up to 255), at least 1."""
+        return self.filter_only_count_hint_from_counter_histogram(self.counter_histogram(), 255)
+
+    def filter_only_count_hint_from_counter_histogram(self, counter_histogram, max_abundance: int) -> int:
+        """src/api.rs:375-385."""
+        dec = _deconvolved_counts(counter_histogram, int(self._cfg.n_hashes), int(max_abundance))
+        return max(_round_u64(_sum_f64(dec)), 1)
 
     def spectrum_distinct(self, data: np.ndarray, offsets: np.ndarray) -> dict:
         """estimate_distinct_kmers + spectrum_from_estimates (fastx.rs:255-308, 392-410)."""
