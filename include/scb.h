@@ -238,6 +238,19 @@ scb_status scb_graph_stats(const scb_ctx* ctx, uint64_t* captures, uint64_t* rep
  * the grouped strategy; results are identical to one batch. */
 scb_status scb_set_piece_bytes(scb_ctx* ctx, uint64_t piece_bytes);
 
+/* Host FASTA/FASTQ reader (replaces the reference's parser thread feeding the workers,
+ * src/api.rs:621-674, with its record rules, src/api.rs:893-915): reads a plain or gzip file in
+ * one pass into concatenated sequences with n_records + 1 offsets (the layout of
+ * scb_insert_batch) and the records' header lines.  Host memory only; no GPU needed.  The
+ * pointers stay valid until scb_fastx_free.  A file that cannot be opened fails with
+ * SCB_ERR_FASTX_OPEN. */
+typedef struct scb_fastx scb_fastx;
+scb_status scb_fastx_read(const char* path, scb_fastx** out);
+scb_status scb_fastx_sequences(const scb_fastx* f, const uint8_t** seqs, const uint64_t** offsets,
+                               uint64_t* n_records);
+scb_status scb_fastx_headers(const scb_fastx* f, const uint8_t** headers, const uint64_t** header_offsets);
+void scb_fastx_free(scb_fastx* f);
+
 /* ---------------------------------------------------------------------------------------
  * Serving: a request loop over a frozen, device-resident index (no counterpart in the
  * reference, whose queries run per call; this batches SuperCountingBloomIndex::

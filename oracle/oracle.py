@@ -429,3 +429,42 @@ def filter_only_count_hint(counter_histogram, n_hashes: int, max_abundance: int 
     """src/api.rs:375-385 (filter_only_count_hint_from_counter_histogram)."""
     s = _sum_left(filter_only_deconvolved_counts(counter_histogram, n_hashes, max_abundance))
     return max(rust_round_u64(s), 1)
+
+
+# ---------------------------------------------------------------------------------------
+# FASTA/FASTQ records (src/api.rs:893-915): the line-by-line reader, the checker of the library's
+# one-pass reader (scb_fastx_read).  Lines end at b"\n" and lose trailing b"\r" / b"\n"; b">" or
+# b"@" opens a record; a FASTQ record's sequence runs to a b"+" line and the next line (its
+# qualities) is skipped; lines before the first header are ignored; gzip input is inflated.
+# ---------------------------------------------------------------------------------------
+def fastx_records(path: str):
+    """Yields (header without its marker, sequence) per record."""
+    import gzip
+
+    with open(path, "rb") as probe:
+        gz = probe.read(2) == b"\x1f\x8b"
+    with (gzip.open(path, "rb") if gz else open(path, "rb")) as fh:
+        header = None
+        seq: list[bytes] = []
+        fastq_state = 0
+        for raw in fh:
+            line = raw.rstrip(b"\r\n")
+            if fastq_state == 2:
+                fastq_state = 0
+                continue
+            if fastq_state == 1:
+                if line.startswith(b"+"):
+                    fastq_state = 2
+                else:
+                    seq.append(line)
+                continue
+            if line.startswith(b">") or line.startswith(b"@"):
+                if header is not None:
+                    yield header, b"".join(seq)
+                header = line[1:]
+                seq = []
+                fastq_state = 1 if line.startswith(b"@") else 0
+            elif header is not None:
+                seq.append(line)
+        if header is not None:
+            yield header, b"".join(seq)

@@ -137,6 +137,10 @@ def load(path: str | None = None):
         "scb_get_timings": (C.c_int, [ctxp, C.POINTER(ScbTimings)]),
         "scb_set_graphs": (C.c_int, [ctxp, C.c_int]),
         "scb_set_piece_bytes": (C.c_int, [ctxp, C.c_uint64]),
+        "scb_fastx_read": (C.c_int, [C.c_char_p, C.POINTER(vp)]),
+        "scb_fastx_sequences": (C.c_int, [vp, C.POINTER(vp), C.POINTER(vp), u64p]),
+        "scb_fastx_headers": (C.c_int, [vp, C.POINTER(vp), C.POINTER(vp)]),
+        "scb_fastx_free": (None, [vp]),
         "scb_graph_stats": (C.c_int, [ctxp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
         "scb_reset": (C.c_int, [ctxp]),
         "scb_query_report_device_noalloc": (C.c_int, [ctxp, vp, vp, C.c_uint64, C.c_uint64, vp,

@@ -11,12 +11,11 @@ from __future__ import annotations
 
 import ctypes as C
 import enum
-import gzip
 import math
 import os
 import time
 from dataclasses import dataclass, field
-from typing import Callable, Iterator
+from typing import Callable
 
 import numpy as np
 
@@ -370,45 +369,42 @@ def set_strategy(obj, insert: str = "auto", query: str = "auto") -> None:
 # ---------------------------------------------------------------------------------------
 # FASTA / FASTQ (host parsing; helicase semantics of records and names)
 # ---------------------------------------------------------------------------------------
-def _open_text(path: str):
-    try:
-        fh = open(path, "rb")
-    except OSError as err:
-        raise FastxOpen(f"failed to open FASTA/FASTQ '{path}': {err}") from err
-    head = fh.read(2)
-    fh.seek(0)
-    if head == b"\x1f\x8b":
-        fh.close()
-        return gzip.open(path, "rb")
-    return fh
+class _FastxOwner:
+    """Holds one native read of a FASTA/FASTQ file (scb_fastx_read); the arrays viewing its memory
+    keep it alive, and it is freed with the last of them."""
+
+    def __init__(self, handle):
+        self.h = handle
+
+    def __del__(self):
+        if self.h:
+            _lib.load().scb_fastx_free(self.h)
+            self.h = None
 
 
-def _iter_records(path: str) -> Iterator[tuple[bytes, bytes]]:
-    with _open_text(path) as fh:
-        header = None
-        seq: list[bytes] = []
-        fastq_state = 0
-        for raw in fh:
-            line = raw.rstrip(b"\r\n")
-            if fastq_state == 2:  # FASTQ quality line
-                fastq_state = 0
-                continue
-            if fastq_state == 1:
-                if line.startswith(b"+"):
-                    fastq_state = 2
-                else:
-                    seq.append(line)
-                continue
-            if line.startswith(b">") or line.startswith(b"@"):
-                if header is not None:
-                    yield header, b"".join(seq)
-                header = line[1:]
-                seq = []
-                fastq_state = 1 if line.startswith(b"@") else 0
-            elif header is not None:
-                seq.append(line)
-        if header is not None:
-            yield header, b"".join(seq)
+def _view(owner: _FastxOwner, addr: int, n: int, ctype, dtype) -> np.ndarray:
+    if n == 0 or not addr:
+        return np.zeros(0, dtype)
+    buf = (ctype * n).from_address(addr)
+    buf._owner = owner
+    return np.frombuffer(buf, dtype=dtype)
+
+
+def _fastx_read(path: str) -> tuple[np.ndarray, np.ndarray, np.ndarray, np.ndarray]:
+    """Sequences, offsets (n + 1), headers and header offsets of a FASTA/FASTQ file (plain or gzip),
+    read by the library's one-pass reader without copies."""
+    L = _lib.load()
+    h = C.c_void_p()
+    _check(L.scb_fastx_read(os.fsencode(path), C.byref(h)))
+    owner = _FastxOwner(h)
+    sp, op, hp, hop, n = C.c_void_p(), C.c_void_p(), C.c_void_p(), C.c_void_p(), C.c_uint64()
+    _check(L.scb_fastx_sequences(h, C.byref(sp), C.byref(op), C.byref(n)))
+    _check(L.scb_fastx_headers(h, C.byref(hp), C.byref(hop)))
+    offsets = _view(owner, op.value, n.value + 1, C.c_uint64, np.uint64)
+    hoffs = _view(owner, hop.value, n.value + 1, C.c_uint64, np.uint64)
+    seqs = _view(owner, sp.value, int(offsets[-1]), C.c_uint8, np.uint8)
+    headers = _view(owner, hp.value, int(hoffs[-1]), C.c_uint8, np.uint8)
+    return seqs, offsets, headers, hoffs
 
 
 def _record_name(header: bytes, idx: int) -> str:
@@ -419,14 +415,17 @@ def _record_name(header: bytes, idx: int) -> str:
 
 def for_each_fastx_record(path: str, visit: Callable[[str, bytes], None]) -> None:
     """src/api.rs:893-915."""
-    for i, (header, seq) in enumerate(_iter_records(str(path)), start=1):
-        visit(_record_name(header, i), seq)
+    seqs, offsets, headers, hoffs = _fastx_read(str(path))
+    sv, hv = memoryview(seqs), memoryview(headers)
+    o, ho = offsets.tolist(), hoffs.tolist()
+    for i in range(len(o) - 1):
+        visit(_record_name(bytes(hv[ho[i]:ho[i + 1]]), i + 1), bytes(sv[o[i]:o[i + 1]]))
 
 
 def _read_batch(path: str) -> tuple[np.ndarray, np.ndarray]:
-    seqs = []
-    for_each_fastx_record(path, lambda _n, s: seqs.append(s))
-    return pack_sequences(seqs)
+    """All records of a FASTA/FASTQ file as one batch (concatenated sequences, offsets)."""
+    seqs, offsets, _, _ = _fastx_read(str(path))
+    return seqs, offsets
 
 
 # ---------------------------------------------------------------------------------------

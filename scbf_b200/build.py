@@ -16,7 +16,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libscb_b200.so")
 
-SOURCES = ["scb_api.cu", "scb_kernels.cu", "scb_server.cu"]
+SOURCES = ["scb_api.cu", "scb_kernels.cu", "scb_server.cu", "scb_fastx.cu"]
 HEADERS = ["scb_device.cuh", "scb_kernels.cuh", "scb_internal.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3", "--expt-relaxed-constexpr",
@@ -45,7 +45,7 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
     bdir = os.path.join(HERE, "_build")
     os.makedirs(bdir, exist_ok=True)
     for src in SOURCES:
-        obj = os.path.join(bdir, src.replace(".cu", ".o"))
+        obj = os.path.join(bdir, os.path.splitext(src)[0] + ".o")
         cmd = [nvcc(), *ARCH, *FLAGS, *(extra or []), "-I", os.path.join(ROOT, "include"), "-c",
                os.path.join(CSRC, src), "-o", obj]
         if verbose:
@@ -53,7 +53,7 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
         subprocess.run(cmd, check=True)
         objs.append(obj)
     tmp = LIB + ".tmp"
-    cmd = [nvcc(), *ARCH, "-shared", "-cudart", "static", *objs, "-o", tmp, "-lpthread"]
+    cmd = [nvcc(), *ARCH, "-shared", "-cudart", "static", *objs, "-o", tmp, "-lpthread", "-lz"]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)
