@@ -19,6 +19,8 @@ from dataclasses import dataclass
 
 import numpy as np
 
+MASK64 = (1 << 64) - 1
+
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "libscb_oracle.so")
 
@@ -468,3 +470,54 @@ def fastx_records(path: str):
                 seq.append(line)
         if header is not None:
             yield header, b"".join(seq)
+
+
+# ---------------------------------------------------------------------------------------
+# Sampled spectrum (src/bin/sampled_spectrum.rs:182-223, 263-305): reservoir sampling of the
+# valid k-mer windows, restated as the sequential loop (the checker of the vectorised sampler).
+# ---------------------------------------------------------------------------------------
+def _splitmix_next(state: int) -> tuple[int, int]:
+    state = (state + 0x9E3779B97F4A7C15) & MASK64
+    v = state
+    v = ((v ^ (v >> 30)) * 0xBF58476D1CE4E5B9) & MASK64
+    v = ((v ^ (v >> 27)) * 0x94D049BB133111EB) & MASK64
+    return state, v ^ (v >> 31)
+
+
+def reservoir_sample_kmers(sequences, k: int, capacity: int, seed: int) -> tuple[list[bytes], int]:
+    """The sampled k-mers (upper case, in reservoir slot order) and the number of windows seen."""
+    kmers: list[bytes] = []
+    seen = 0
+    state = seed & MASK64
+    for seq in sequences:
+        if len(seq) < k:
+            continue
+        runs, start = [], None
+        for i, b in enumerate(seq):
+            ub = b - 32 if 97 <= b <= 122 else b  # to_ascii_uppercase
+            if ub in (65, 67, 71, 84):
+                if start is None:
+                    start = i
+            elif start is not None:
+                runs.append((start, i))
+                start = None
+        if start is not None:
+            runs.append((start, len(seq)))
+        for a, e in runs:
+            if e - a < k:
+                continue
+            for off in range(a, e - k + 1):
+                seen += 1
+                if len(kmers) < capacity:
+                    slot = len(kmers)
+                else:
+                    state, v = _splitmix_next(state)
+                    r = v % seen
+                    slot = r if r < capacity else None
+                if slot is not None:
+                    km = seq[off:off + k].upper()
+                    if slot == len(kmers):
+                        kmers.append(km)
+                    else:
+                        kmers[slot] = km
+    return kmers, seen

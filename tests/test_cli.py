@@ -1,6 +1,7 @@
-"""The command-line tools (src/bin/build-index.rs, query-index.rs, filter_spectrum.rs): the
-reference's arguments and error exits on the host, and on the GPU the same index bytes, CSV rows
-and spectrum as the library calls they wrap."""
+"""The command-line tools (src/bin/build-index.rs, query-index.rs, filter_spectrum.rs,
+sampled_spectrum.rs): the reference's arguments and error exits, the sampled spectrum's reservoir
+and scaling against the oracle's sequential restatement on the host, and on the GPU the same index
+bytes, CSV rows and spectrum as the library calls they wrap."""
 import csv
 import io
 import os
@@ -109,3 +110,62 @@ def test_tools_match_the_library(tmp_path, capsys, oracle_mod):
     est = idx.estimate_filter_only_spectrum_from_counter_histogram(hist, 40, hint)
     assert rows[0] == ["estimated_count", "estimated_kmers", "method", "kmer_count_hint"]
     assert rows[1:] == [[str(a), str(n), est.method, str(hint)] for a, n in est.rows]
+
+
+def _random_batch(rng, n_seqs, k):
+    seqs = []
+    for _ in range(n_seqs):
+        L = int(rng.integers(0, 3 * k))
+        s = bytearray(rng.choice(np.frombuffer(b"ACGTacgtNn", np.uint8), L, p=[.2, .2, .2, .2, .04, .04, .04, .04,
+                                                                               .02, .02]).tobytes())
+        seqs.append(bytes(s))
+    return seqs
+
+
+@pytest.mark.parametrize("k,capacity,seed,chunk", [(5, 1, 1, 64), (7, 4, 0, 5), (9, 37, (1 << 64) - 1, 1 << 24),
+                                                   (11, 10**6, 12345, 13), (5, 200, 7, 1000)])
+def test_reservoir_sample_matches_sequential_sampler(oracle_mod, k, capacity, seed, chunk):
+    """The vectorised reservoir (counter-based SplitMix64 calls, chunked windows) keeps exactly the
+    k-mers of the sequential sampler of src/bin/sampled_spectrum.rs, in the same slots."""
+    import scbf_b200 as scb
+
+    rng = np.random.default_rng(k * 1000 + capacity)
+    seqs = _random_batch(rng, 400, k)
+    data, offsets = scb.pack_sequences(seqs)
+    kmers, seen = cli.sample_kmers(data, offsets, k, capacity, seed, chunk=chunk)
+    want, want_seen = oracle_mod.reservoir_sample_kmers(seqs, k, capacity, seed)
+    assert seen == want_seen
+    assert [bytes(r) for r in kmers] == want
+
+
+def test_sampled_rows_match_literal_histogram(oracle_mod):
+    """The batch query of the sample and the scaling of sampled_spectrum.rs:225-261, with the
+    oracle as the estimator, against per-k-mer queries and Rust rounding."""
+    import scbf_b200 as scb
+
+    rng = np.random.default_rng(4)
+    genome = rng.choice(np.frombuffer(b"ACGT", np.uint8), 3000).tobytes()
+    seqs = [genome[s:s + 60] for s in rng.integers(0, 2940, 300)]
+    data, offsets = scb.pack_sequences(seqs)
+    o = oracle_mod.OracleFilter(oracle_mod.make_config(11, 7, 9, 3, 8, 14, 6, 1, 4))
+    o.insert_batch_arrays(data, offsets)
+    kmers, seen = cli.sample_kmers(data, offsets, 11, 500, 3)
+    rows, invalid = cli.sampled_rows(kmers, seen, o.query_batch_arrays)
+    hist = {}
+    for km in kmers:
+        v = o.estimate_sequence_abundances(bytes(km))[0]
+        hist[v] = hist.get(v, 0) + 1
+    scale = float(seen) / float(len(kmers))
+    want = []
+    for a in sorted(hist):
+        lsw = oracle_mod.rust_round_u64(float(hist[a]) * scale)
+        want.append((a, hist[a], lsw, 0 if a == 0 else oracle_mod.rust_round_u64(float(lsw) / float(a))))
+    assert invalid == 0 and rows == want
+
+
+def test_sampled_spectrum_rejects_empty_sample(tmp_path, capsys):
+    fa = _fasta(tmp_path / "r.fa", n=3)
+    assert cli.main(["sampled-spectrum", str(fa), "--sample-size", "0"]) == 1
+    assert "error: invalid config: sample_size must be positive" in capsys.readouterr().err
+    with pytest.raises(SystemExit):
+        cli.main(["sampled-spectrum", str(fa), "--seed", "-1"])
