@@ -378,7 +378,10 @@ class _FastxOwner:
 
     def __del__(self):
         if self.h:
-            _lib.load().scb_fastx_free(self.h)
+            try:
+                _lib.load().scb_fastx_free(self.h)
+            except Exception:  # interpreter shutdown: the process frees its memory anyway
+                pass
             self.h = None
 
 
