@@ -8,6 +8,7 @@
 // one line after that, the qualities, is skipped); other lines extend the open record's sequence;
 // lines before the first header are ignored.  A file starting with the gzip magic is inflated
 // (concatenated members included).
+#include <sys/stat.h>
 #include <zlib.h>
 
 #include <cerrno>
@@ -60,6 +61,11 @@ struct Offsets {
 };
 
 scb_status read_file(const char* path, Bytes& out) {
+    struct stat st;
+    if (::stat(path, &st) == 0 && S_ISDIR(st.st_mode)) {
+        return scb::fail(SCB_ERR_FASTX_OPEN,
+                         std::string("failed to open FASTA/FASTQ '") + path + "': " + std::strerror(EISDIR));
+    }
     FILE* fp = std::fopen(path, "rb");
     if (!fp) {
         return scb::fail(SCB_ERR_FASTX_OPEN,

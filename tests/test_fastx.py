@@ -63,6 +63,8 @@ def test_batch_layout_and_names(tmp_path):
     assert names == ["contig_1", "contig_2", "record_3"] and seqs == [b"ACGTNN", b"TGCATG", b"A"]
 
 
-def test_missing_file_is_fastx_open(tmp_path):
+def test_missing_file_or_directory_is_fastx_open(tmp_path):
     with pytest.raises(api.FastxOpen):
         api._fastx_read(str(tmp_path / "none.fa"))
+    with pytest.raises(api.FastxOpen):
+        api._fastx_read(str(tmp_path))
