@@ -142,13 +142,16 @@ scb_status scb_query_report_device(scb_ctx* ctx, const uint8_t* d_seqs, const ui
                                    uint64_t n_seqs, uint64_t n_bytes, void* stream, scb_report* report);
 
 /* No counterpart in the reference.  scb_query_report_device without any device allocation, for
- * callers that cannot allocate while they run: code inside a CUDA stream capture, real-time
- * serving threads that keep the allocator out of the request path, hosts that give the library a
- * fixed memory budget.  Its scratch is one static device array of about 16 MiB that every GPU
- * loading this library holds until exit; batches are limited to 32 MiB of sequence bytes (larger
- * ones fail with SCB_ERR_INTERNAL_STATE).  The first call on a device looks up the array's
- * address; make that first call before any stream capture.  All calls share the array (each
- * clears what it reads), so calls whose GPU work overlaps race: serialise them. */
+ * callers that cannot call cudaMalloc while they run: real-time serving threads that keep the
+ * allocator's latency and its device-wide synchronisation out of the request path, and hosts
+ * that hand the library a fixed device-memory budget at start-up and account for every byte.  Its
+ * scratch is one static device array of about 16 MiB that every GPU loading this library holds
+ * until the process exits; batches are limited to 32 MiB of sequence bytes (larger ones fail
+ * with SCB_ERR_INTERNAL_STATE before any work).  The first call on a device looks up the array's
+ * device address with that device current and keeps it for the life of the process, so a
+ * process that resets the device (cudaDeviceReset) must not call this entry point afterwards.
+ * The call ends by reading the report back and synchronising the stream.  All calls share the
+ * array (each clears what it reads), so calls whose GPU work overlaps race: serialise them. */
 scb_status scb_query_report_device_noalloc(scb_ctx* ctx, const uint8_t* d_seqs, const uint64_t* d_offsets,
                                            uint64_t n_seqs, uint64_t n_bytes, void* stream, scb_report* report);
 
@@ -184,6 +187,10 @@ scb_status scb_load(const char* path, scb_ctx** out);
  * (src/filter.rs:575-605). bytes must equal 2^counter_slots_exponent * counter_bits / 8. */
 uint64_t scb_table_bytes(const scb_ctx* ctx);
 scb_status scb_table_download(const scb_ctx* ctx, void* host, uint64_t bytes);
+/* The same bytes in pieces: table bytes [offset, offset + bytes) (write_counter_data streams
+ * shard by shard, src/filter.rs:575-580), so a caller can save or compare a table of up to
+ * 16 GiB without holding it whole in host memory. */
+scb_status scb_table_download_range(const scb_ctx* ctx, uint64_t offset, void* host, uint64_t bytes);
 scb_status scb_table_upload(scb_ctx* ctx, const void* host, uint64_t bytes, uint64_t inserted_kmers);
 
 /* Strategy control and workload statistics. */

@@ -78,6 +78,7 @@ def lib():
         L.ora_filter_new.restype = vp
         L.ora_filter_new.argtypes = [C.POINTER(OraConfig)]
         L.ora_filter_free.argtypes = [vp]
+        L.ora_filter_clear.argtypes = [vp]
         L.ora_filter_table.restype = vp
         L.ora_filter_table.argtypes = [vp]
         L.ora_filter_table_bytes.restype = C.c_uint64
@@ -198,6 +199,16 @@ class OracleFilter:
             self.close()
         except Exception:
             pass
+
+    def clear(self):
+        """All counters and totals back to zero on the same (already touched) allocation."""
+        lib().ora_filter_clear(self.h)
+
+    def table_view(self) -> np.ndarray:
+        """The table's bytes without a copy (valid while the filter lives)."""
+        L = lib()
+        nbytes = L.ora_filter_table_bytes(self.h)
+        return np.frombuffer((C.c_uint8 * nbytes).from_address(L.ora_filter_table(self.h)), dtype=np.uint8)
 
     @property
     def counter_bits(self) -> int:

@@ -73,6 +73,7 @@ size_t ora_super_kmers(const uint8_t* codes, size_t len, size_t k, size_t m, uin
 /* Filter lifecycle (filter.rs:118-145).  The counter table is kept in file order. */
 ora_filter* ora_filter_new(const ora_config* cfg);
 void ora_filter_free(ora_filter* f);
+void ora_filter_clear(ora_filter* f);
 void* ora_filter_table(ora_filter* f);
 uint64_t ora_filter_table_bytes(const ora_filter* f);
 uint64_t ora_filter_inserted_kmers(const ora_filter* f);

@@ -128,6 +128,7 @@ def load(path: str | None = None):
         "scb_load": (C.c_int, [C.c_char_p, C.POINTER(ctxp)]),
         "scb_table_bytes": (C.c_uint64, [ctxp]),
         "scb_table_download": (C.c_int, [ctxp, vp, C.c_uint64]),
+        "scb_table_download_range": (C.c_int, [ctxp, C.c_uint64, vp, C.c_uint64]),
         "scb_table_upload": (C.c_int, [ctxp, vp, C.c_uint64, C.c_uint64]),
         "scb_set_strategy": (C.c_int, [ctxp, C.c_int, C.c_int]),
         "scb_get_strategy": (C.c_int, [ctxp, C.POINTER(C.c_int), C.POINTER(C.c_int)]),

@@ -1711,6 +1711,20 @@ scb_status scb_table_download(const scb_ctx* cctx, void* host, uint64_t bytes) {
     return SCB_OK;
 }
 
+scb_status scb_table_download_range(const scb_ctx* cctx, uint64_t offset, void* host, uint64_t bytes) {
+    if (!cctx || (!host && bytes)) return fail_kind(SCB_ERR_INTERNAL_STATE, "null argument");
+    scb_ctx* ctx = const_cast<scb_ctx*>(cctx);
+    CtxLock lk(ctx);
+    if (offset > ctx->table_bytes || bytes > ctx->table_bytes - offset) {
+        return fail_kind(SCB_ERR_INTERNAL_STATE, "range [" + std::to_string(offset) + ", +" + std::to_string(bytes) +
+                                                     ") is outside the " + std::to_string(ctx->table_bytes) +
+                                                     "-byte table");
+    }
+    if (bytes) SCB_CUDA(cudaMemcpy(host, static_cast<const uint8_t*>(ctx->table) + offset, bytes,
+                                   cudaMemcpyDeviceToHost));
+    return SCB_OK;
+}
+
 scb_status scb_table_upload(scb_ctx* ctx, const void* host, uint64_t bytes, uint64_t inserted_kmers) {
     if (!ctx || !host) return fail_kind(SCB_ERR_INTERNAL_STATE, "null argument");
     CtxLock lk(ctx);
@@ -2057,17 +2071,19 @@ scb_status scb_autotune(scb_ctx* ctx, const uint8_t* seqs, const uint64_t* offse
 // ---------------------------------------------------------------------------------------
 // Allocation-free query report.
 //
-// For callers that must not allocate device memory while they run: code inside a CUDA stream
-// capture (cudaMalloc is not a stream operation and breaks the capture), real-time serving
-// threads that keep allocator latency and fragmentation out of the request path, and hosts that
-// hand this library a fixed memory budget at start-up.  The per-call scratch of the fused
-// report query (2-bit codes, ACGT and sequence-start bitmaps, counters, the tile work counter)
-// lives in one file-scope device array instead of buffers allocated per call.
+// For callers that must not call cudaMalloc while they run: real-time serving threads that keep
+// the allocator's latency (and the device-wide synchronisation cudaMalloc / cudaFree can imply)
+// out of the request path, and hosts that hand this library a fixed device-memory budget at
+// start-up.  The per-call scratch of the fused report query (2-bit codes, ACGT and
+// sequence-start bitmaps, counters, the tile work counter) lives in one file-scope device array
+// instead of buffers allocated per call.
 //
 // Limits: batches of at most kNoallocMaxBytes sequence bytes.  The array takes
-// kNoallocScratchBytes on every GPU that loads this library, until the process exits.  All calls
-// share it: the call clears what must start at zero, and two calls whose work overlaps on the
-// GPU (different streams or threads) race on it, so such callers serialise their calls.
+// kNoallocScratchBytes on every GPU that loads this library, until the process exits.  Its
+// device address is looked up once per device (with that device current) and kept, so the
+// entry point must not be used after a cudaDeviceReset of that device.  All calls share the
+// array: the call clears what must start at zero, and two calls whose work overlaps on the GPU
+// (different streams or threads) race on it, so such callers serialise their calls.
 // ---------------------------------------------------------------------------------------
 namespace {
 
