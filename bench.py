@@ -40,7 +40,8 @@ METRIC = "k-mers/s (build + stream query)"
 WORKLOAD = ("default geometry, short reads: 100 Mbp uniform genome, 20x of 150 bp reads (13.3M reads, 2 Gbp), "
             "both strands, 1% substitutions, 1% of bases N in runs of 1-10; k=31 m=21 s=25 h=4, 16-bit "
             "counters, 2^30 slots (2 GiB), 2^9 slots per block")
-CPU_SAMPLE_READS = 200_000
+CPU_SAMPLE_READS = 2_000_000  # the CPU-baseline leg of our arm: one timed run
+REF_STEP_READS = 1_000_000  # the reference arm: reads per step
 
 
 def parse():
@@ -183,6 +184,17 @@ def measured_peaks() -> tuple[float, str]:
         return 6650.0, "fallback"
 
 
+def kernel_source_hash() -> str:
+    """Hash of the CUDA sources (the kernels a committed ncu capture measured)."""
+    import hashlib
+
+    h = hashlib.sha256()
+    for name in ("scb_kernels.cu", "scb_kernels.cuh", "scb_device.cuh"):
+        with open(os.path.join(ROOT, "scbf_b200", "csrc", name), "rb") as fh:
+            h.update(fh.read())
+    return h.hexdigest()[:16]
+
+
 def profile_traffic() -> dict | None:
     """Per-kernel DRAM bytes per launch of the grouped step on this workload, from the committed
     one-pass ncu capture (profiles/traffic_grouped_config2.json), with the pipe that limits each
@@ -201,36 +213,60 @@ def workload(rank: int, scale: float):
 
 
 # ---------------------------------------------------------------------------------------
+def cpu_port_run(data, offsets, first: int, reads: int, f) -> tuple[float, int, str]:
+    """The CPU port (reference structure: parser thread, bounded queue of 4096, all host threads,
+    1024 mutex shards) on reads [first, first + reads) of the workload, on filter f after a clear:
+    f's table was touched before, so the timed region holds build + stream query work only."""
+    n_total = len(offsets) - 1
+    a = first % n_total
+    b = min(a + reads, n_total)
+    so = (offsets[a:b + 1] - offsets[a]).astype(np.uint64)
+    sd = data[int(offsets[a]):int(offsets[b])]
+    threads = os.cpu_count() or 1
+    f.clear()
+    t0 = time.perf_counter()
+    r = f.port_build_and_stream_query(sd, so, threads=threads, queue=4096)
+    dt = time.perf_counter() - t0
+    return dt, r["inserted_kmers"], f"reads {a}..{b}"
+
+
+def cpu_filter():
+    from oracle import oracle
+
+    threads = os.cpu_count() or 1
+    f = oracle.OracleFilter(oracle.make_config(GEOM["k"], GEOM["m"], GEOM["s"], GEOM["n_hashes"], GEOM["counter_bits"],
+                                               GEOM["counter_slots_exponent"], GEOM["block_slots_exponent"], threads,
+                                               4096))
+    f.clear()  # first touch of every page of the 2 GiB table, outside any timed region
+    return f, threads
+
+
 def run_reference(args, dist: Dist):
     if dist.rank != 0:
         return
-    from oracle import oracle
-
     data, offsets = workload(0, args.scale)
-    n = min(CPU_SAMPLE_READS, len(offsets) - 1)
-    so = offsets[: n + 1].copy()
-    sd = data[: int(so[-1])]
-    threads = os.cpu_count() or 1
-    cfg = oracle.make_config(GEOM["k"], GEOM["m"], GEOM["s"], GEOM["n_hashes"], GEOM["counter_bits"],
-                             GEOM["counter_slots_exponent"], GEOM["block_slots_exponent"], threads, 4096)
+    n_total = len(offsets) - 1
+    per_step = min(REF_STEP_READS, n_total)
+    f, threads = cpu_filter()
     times, kmers = [], 0
     for step in range(args.warmup + args.steps):
-        f = oracle.OracleFilter(cfg)
-        t0 = time.perf_counter()
-        r = f.port_build_and_stream_query(sd, so, threads=threads, queue=4096)
-        dt = time.perf_counter() - t0
-        f.close()
-        kmers = r["inserted_kmers"]
+        # consecutive steps take consecutive slices, so the timed steps cover the whole workload
+        dt, km, _ = cpu_port_run(data, offsets, step * per_step, per_step, f)
         if step >= args.warmup:
             times.append(dt)
+            kmers += km
+    f.close()
     total = sum(times)
-    value = kmers * len(times) / total
-    sample = f"first {n} reads ({kmers} k-mers) of the workload per step, fresh 2 GiB table each step"
+    value = kmers / total
+    sample = (f"{per_step} reads per step, consecutive slices of the workload ({args.steps} timed steps, "
+              f"{kmers} k-mers in all); each step clears a pre-touched 2 GiB table outside its timed region")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "k-mers/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "sample": sample, "parallelism": f"{threads} host threads"},
+        "config": {"workload": WORKLOAD + (f" (genome scale {args.scale})" if args.scale != 1.0 else ""),
+                   "reads": n_total, "bytes": int(offsets[-1]), "sample": sample,
+                   "parallelism": f"{threads} host threads", "strategy": "CPU port of the reference pipeline"},
         "cpu_baseline": {"value": value, "unit": "k-mers/s", "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "k-mers/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -379,65 +415,92 @@ def run_ours(args, dist: Dist):
         e2e = {"value": all_kmers * len(times) / sum(times), "unit": "k-mers/s",
                "h2d_bytes_per_step": n_bytes + (n_seqs + 1) * 8, "d2h_bytes_per_step": 2 * (16 * 8 + 4) + 8}
 
-    # roofline of the dominant kernel of the timed step.  Algorithmic bytes follow the
-    # random-32-byte-sector model of the direct design: each distinct sector that a super-k-mer's
-    # probes hit is read (and, for an insert, written) once per super-k-mer, plus the 2-bit
-    # packed reads; the report query writes no per-window output.  The grouped kernels stage each
-    # touched block once per bucket instead, so they can run above this roofline.
+    # roofline of the dominant kernel of the timed step.  Algorithmic bytes follow the design the
+    # kernel implements: the grouped kernels stage each touched counter block once per bucket, so
+    # their minimum traffic is the sorted records (8 B each), the records' 2-bit bases, and each
+    # touched block read (and, for the insert, written) once; the direct designs (fused tiles)
+    # pay the random-32-byte-sector model (each distinct sector a super-k-mer's probes hit, read
+    # and for the insert written, per super-k-mer).
     peak, peak_kind = measured_peaks()
     R = float(st.super_kmers)
     sector_bytes = 32.0 * st.sectors
     packed = n_bytes / 4.0
-    alg_insert = 2.0 * sector_bytes + packed
-    alg_query = sector_bytes + packed
-    grouped_step = info["cut_ms"] > 0
-    kernels = {
-        "k_apply<insert>": (info["apply_insert_ms"], alg_insert),
-        "k_apply<query>": (info["apply_query_ms"], alg_query),
-        # own bytes of the cut: codes and bitmaps read once, 12-byte record + 8-byte count each
-        "k_tiles<cut>": (info["cut_ms"], n_bytes / 2 + 20 * R),
-        # the fused strategy's tile kernels carry the whole stage
-        "k_tiles<insert>": (0.0 if grouped_step else info["insert_ms"], alg_insert),
-        "k_tiles<report>": (0.0 if grouped_step else info["query_ms"], alg_query),
-    }
-    dom = max(kernels, key=lambda k_: kernels[k_][0])
-    dom_ms, alg = kernels[dom]
-    achieved = alg / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
-    prof = profile_traffic() or {}
-    kprof = prof.get("kernels", {}).get(dom, {})
-    # bytes the grouped design needs at least: sorted records, the gathered bases of each record
-    # (read once), each touched block read (and written, insert) once
+    model_insert = 2.0 * sector_bytes + packed
+    model_query = sector_bytes + packed
     touched = occupied(R, float(1 << (GEOM["counter_slots_exponent"] - GEOM["block_slots_exponent"])))
     block_bytes = (1 << GEOM["block_slots_exponent"]) * (GEOM["counter_bits"] // 8)
     gather = (st.windows + R * (GEOM["k"] - 1)) / 4.0
-    staged_min = {"k_apply<insert>": 8 * R + gather + 2 * touched * block_bytes,
-                  "k_apply<query>": 8 * R + gather + touched * block_bytes}.get(dom)
-
-    def stage(ms, alg_b):
-        gbs = alg_b / (ms / 1e3) / 1e9 if ms > 0 else 0.0
-        return {"ms": ms, "achieved": gbs, "frac": gbs / peak,
-                "kmers_per_s": kmers / (ms / 1e3) if ms > 0 else 0.0,
-                "roofline_kmers_per_s": kmers / (alg_b / (peak * 1e9))}
+    staged_insert = 8 * R + gather + 2 * touched * block_bytes
+    staged_query = 8 * R + gather + touched * block_bytes
+    grouped_step = info["cut_ms"] > 0
+    # (time, algorithmic bytes, random-sector model bytes or None, work units, unit name)
+    kernels = {
+        "k_apply<insert>": (info["apply_insert_ms"], staged_insert, model_insert, float(st.smers), "s-mer"),
+        "k_apply<query>": (info["apply_query_ms"], staged_query, model_query, float(st.smers), "s-mer"),
+        # the cut reads the 2-bit codes and both bitmaps once and writes an 8-byte record and a
+        # 16-byte base entry per super-k-mer
+        "k_tiles<cut>": (info["cut_ms"], n_bytes / 2 + 24 * R, None, float(st.windows), "window"),
+        # pack: ASCII read once, codes (2 bits) and the two bitmaps (1 bit each) written
+        "k_pack": (info["pack_ms"], n_bytes * 1.5, None, float(n_bytes), "base"),
+        "k_tiles<insert>": (0.0 if grouped_step else info["insert_ms"], model_insert, model_insert,
+                            float(st.smers), "s-mer"),
+        "k_tiles<report>": (0.0 if grouped_step else info["query_ms"], model_query, model_query,
+                            float(st.smers), "s-mer"),
+    }
+    dom = max((k_ for k_ in kernels if k_ != "k_pack"), key=lambda k_: kernels[k_][0])
+    dom_ms, alg, model, units, unit = kernels[dom]
+    achieved = alg / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
+    prof = profile_traffic() or {}
+    kprof = prof.get("kernels", {}).get(dom, {})
+    src_hash = kernel_source_hash()
+    fresh = bool(kprof) and prof.get("source_hash") == src_hash
+    step_bytes = sum(v[1] for v in kernels.values() if v[0] > 0)
+    step_s = ms / args.steps / 1e3
+    issue = None
+    if fresh and kprof.get("warp_instructions_per_unit"):
+        # instruction-issue roofline: 4 schedulers x 148 SMs issue one warp instruction per clock
+        wipu = kprof["warp_instructions_per_unit"]
+        sm_mhz = info["clocks"].get("sm_mhz") or 1965.0
+        issue_rate = 4 * 148 * sm_mhz * 1e6
+        issue = {"unit": unit, "warp_instructions_per_unit": wipu,
+                 "thread_instructions_per_unit": 32 * wipu,
+                 "floor_thread_instructions_per_unit": kprof.get("floor_thread_instructions_per_unit"),
+                 "floor_note": kprof.get("floor_note"),
+                 "issue_bound_ms": units * wipu / issue_rate * 1e3,
+                 "frac": (units * wipu / issue_rate) / (dom_ms / 1e3) if dom_ms > 0 else None,
+                 "source": prof.get("source_small")}
 
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_kind": peak_kind,
-                "traffic": kprof.get("dram_bytes_per_launch"),
-                "traffic_source": prof.get("source") if kprof else None,
-                # what HBM actually carried: the measured DRAM bytes of a launch over its time
-                "traffic_frac": (kprof["dram_bytes_per_launch"] / (dom_ms / 1e3) / 1e9 / peak)
-                if kprof.get("dram_bytes_per_launch") and dom_ms > 0 else None,
                 "algorithmic_bytes": alg, "kernel_ms": dom_ms,
-                "algorithmic_model": "random 32-byte sectors: 32 B x distinct sectors per super-k-mer "
-                                     "(x2 for insert) + 2-bit packed reads",
-                "limiter": kprof.get("limiter"),
-                "staged_minimum_bytes": staged_min,
-                "staged_minimum_frac": (staged_min / (dom_ms / 1e3) / 1e9 / peak) if staged_min and dom_ms > 0
-                else None,
-                "stages": {"insert": stage(info["insert_ms"], alg_insert),
-                           "query": stage(info["query_ms"], alg_query)},
-                "kernels_ms": {k_: v[0] for k_, v in kernels.items()},
+                "algorithmic_model": ("grouped design minimum: 8 B record + 2-bit bases per super-k-mer, each "
+                                      "touched 1 KiB block read (and written, insert) once"
+                                      if dom.startswith("k_apply") else
+                                      "direct design: 32 B per distinct sector per super-k-mer (x2 insert) + "
+                                      "2-bit reads"),
+                # measured DRAM bytes per launch from the committed ncu capture, only while the
+                # kernel sources are the ones that capture measured
+                "traffic": kprof.get("dram_bytes_per_launch") if fresh else None,
+                "traffic_source": (prof.get("source") if fresh else
+                                   f"stale or absent (capture of sources {prof.get('source_hash')}, "
+                                   f"these are {src_hash})"),
+                "traffic_frac": (kprof["dram_bytes_per_launch"] / (dom_ms / 1e3) / 1e9 / peak)
+                if fresh and kprof.get("dram_bytes_per_launch") and dom_ms > 0 else None,
+                "limiter": kprof.get("limiter") if fresh else None,
+                "issue": issue,
+                "random_sector_model": None if model is None else {
+                    "bytes": model, "frac": model / (dom_ms / 1e3) / 1e9 / peak if dom_ms > 0 else None,
+                    "note": "the per-super-k-mer sector model of a direct design; the grouped kernels stage "
+                            "each block once per bucket and are not bound by it"},
+                # every kernel's algorithmic bytes of one step over the step time: at most the peak
+                "step_check": {"algorithmic_bytes": step_bytes, "gbs": step_bytes / step_s / 1e9,
+                               "frac": step_bytes / step_s / 1e9 / peak},
+                "kernels": {k_: {"ms": v[0], "algorithmic_bytes": v[1],
+                                 "frac": (v[1] / (v[0] / 1e3) / 1e9 / peak) if v[0] > 0 else None}
+                            for k_, v in kernels.items() if v[0] > 0},
                 "sectors_per_superkmer": st.sectors / max(st.super_kmers, 1),
-                "super_kmers": st.super_kmers, "smers": st.smers, "touched_blocks": touched}
+                "super_kmers": st.super_kmers, "smers": st.smers, "windows": st.windows,
+                "touched_blocks": touched}
 
     del d_data, d_off
     serving = None
@@ -449,21 +512,13 @@ def run_ours(args, dist: Dist):
 
     cpu = None
     if not args.no_cpu and dist.rank == 0 and dist.world == 1:
-        from oracle import oracle
-
         n = min(CPU_SAMPLE_READS, n_seqs)
-        so = offsets[: n + 1].copy()
-        sd = data[: int(so[-1])]
-        threads = os.cpu_count() or 1
-        f = oracle.OracleFilter(oracle.make_config(GEOM["k"], GEOM["m"], GEOM["s"], GEOM["n_hashes"],
-                                                   GEOM["counter_bits"], GEOM["counter_slots_exponent"],
-                                                   GEOM["block_slots_exponent"], threads, 4096))
-        t0 = time.perf_counter()
-        r = f.port_build_and_stream_query(sd, so, threads=threads, queue=4096)
-        dt = time.perf_counter() - t0
+        f, threads = cpu_filter()
+        dt, ckm, _ = cpu_port_run(data, offsets, 0, n, f)
         f.close()
-        cpu = {"value": r["inserted_kmers"] / dt, "unit": "k-mers/s", "cores": threads, "kind": "port",
-               "sample": f"first {n} reads ({r['inserted_kmers']} k-mers), build + stream query, fresh table"}
+        cpu = {"value": ckm / dt, "unit": "k-mers/s", "cores": threads, "kind": "port",
+               "sample": f"first {n} reads ({ckm} k-mers), build + stream query, on a cleared, pre-touched "
+                         f"2 GiB table (no page faults in the timed region)"}
 
     if dist.rank == 0:
         line = {

@@ -25,7 +25,9 @@ enum TileMode : int {
     kModeDebugMin = 5,     // (b) only: chosen minimizer position per window
     kModeMaterialize = 6,  // (b) for the plain pipeline: per-window block id + end flag in HBM
     kModeInsertStaged = 7, // (b)+(c)+(d) with one warp per super-k-mer staging block deltas
-    kModeCut = 8           // (b) for the grouped pipeline: one record per super-k-mer + bucket counts
+    kModeCut = 8,          // (b) for the grouped pipeline: one record per super-k-mer + bucket counts
+    kModeBuild = 9         // grouped apply of a build + stream query: insert a bucket's records, commit,
+                           // then answer the same records' query from the committed shared-memory block
 };
 
 // Sizes and input pointers of one batch, in device memory: a graph captured for a shape class
@@ -49,6 +51,9 @@ constexpr uint32_t kItemRecords = 4096;    // records per work item (heavier buc
 constexpr uint32_t kApplyChunk = 256;      // records staged in shared memory at a time (<= CTA width)
 constexpr uint32_t kMaxBucketSlots = 16384;  // counters of one bucket held in shared memory
 constexpr uint32_t kApplyMaxThreads = 512;
+// s-mers of one work item whose probe slots a build apply keeps in shared memory between its
+// insert and its query (items with more are deferred to the query kernel)
+constexpr uint32_t kKeptSmers = 8192;
 
 struct GroupArgs {
     DevGeom g;
@@ -77,6 +82,13 @@ struct GroupArgs {
     unsigned long long* item_base;
     unsigned long long* probe_count;
     uint64_t probe_cap;
+    // build apply (kModeBuild): the report counters of the items it answers itself, and the list
+    // of items it leaves to the query kernel (split buckets, items of more than kKeptSmers
+    // s-mers) with their probe-slot bases; dcount counts them
+    unsigned long long* qcnt;
+    uint4* ditems;
+    unsigned long long* ditem_base;
+    unsigned long long* dcount;
 };
 constexpr unsigned long long kNoProbes = ~0ull;
 

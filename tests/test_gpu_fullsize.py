@@ -121,7 +121,7 @@ def test_config1_exact_against_oracle(scb, oracle_mod):
 def test_config2_full_size_against_cpu_port(scb, oracle_mod):
     import torch
 
-    from scbf_b200 import _lib, workloads
+    from scbf_b200 import _lib, api, workloads
 
     if _host_bytes_available() < 12 * GIB:
         pytest.skip("needs about 8 GiB of free host memory")
@@ -133,6 +133,15 @@ def test_config2_full_size_against_cpu_port(scb, oracle_mod):
     pres = port.port_build_and_stream_query(data, offsets, threads=threads, queue=4096)
     ref = port.table_view()
     assert pres["inserted_kmers"] > 1_400_000_000
+    # the port reports the stream query's own units (src/fastx.rs:310-369): chunks (maximal ACGT
+    # runs of at least k bases) and their windows; the C ABI reports QueryFastaReport's: records
+    # and all their windows, of which valid_kmers are queried
+    chunks, chunk_windows = api._chunk_stats(data, offsets, 31)
+    pr = pres["report"]
+    assert (pr.records_processed, pr.total_windows, pr.valid_kmers) == (chunks, chunk_windows, chunk_windows)
+    lens = np.diff(offsets.astype(np.int64))
+    expect = (n, int(np.where(lens >= 31, lens - 30, 0).sum()), pr.valid_kmers, pr.positive_estimates,
+              pr.estimate_checksum)
 
     L = _lib.load()
     b = scb.SuperCountingBloomBuilder(_cfg(scb, 16, 30))
@@ -143,7 +152,7 @@ def test_config2_full_size_against_cpu_port(scb, oracle_mod):
     assert L.scb_build_and_stream_query(h, data.ctypes.data, offsets.ctypes.data, n, C.byref(km), C.byref(sm),
                                         C.byref(r)) == 0, _lib.last_error()
     assert (km.value, sm.value) == (pres["inserted_kmers"], pres["inserted_smers"])
-    assert _report_tuple(r) == _report_tuple(pres["report"])
+    assert _report_tuple(r) == expect
     _assert_table_equal(L, h, ref)
 
     # device entry point on resident reads (the benchmark's timed call), after a reset
@@ -154,7 +163,7 @@ def test_config2_full_size_against_cpu_port(scb, oracle_mod):
                                                C.byref(km), C.byref(sm), C.byref(r)) == 0, _lib.last_error()
     torch.cuda.synchronize()
     assert (km.value, sm.value) == (pres["inserted_kmers"], pres["inserted_smers"])
-    assert _report_tuple(r) == _report_tuple(pres["report"])
+    assert _report_tuple(r) == expect
     _assert_table_equal(L, h, ref)
 
 
