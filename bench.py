@@ -392,6 +392,19 @@ def run_ours(args, dist: Dist):
         strategies[name] = {"value": all_kmers * s_steps / (sms / 1e3), "ms_per_step": sms / s_steps,
                             "insert_ms": sinfo["insert_ms"], "query_ms": sinfo["query_ms"]}
     check(L.scb_set_strategy(h, 0, 0))
+    if not args.no_plain:
+        # the tuned step with the grouped insert and query as two passes (probe slots stored by the
+        # insert, read back by the query) instead of the build apply that answers each exclusive
+        # bucket right after its commit
+        check(L.scb_set_fused_build(h, 0))
+        s_steps = max(1, args.steps // 2)
+        sms, sinfo = timed("auto", s_steps)
+        check(L.scb_set_fused_build(h, 1))
+        assert sinfo["report"] == reference_report, ("two-pass", sinfo["report"], reference_report)
+        strategies["auto_two_pass"] = {"value": all_kmers * s_steps / (sms / 1e3), "ms_per_step": sms / s_steps,
+                                       "insert_ms": sinfo["insert_ms"], "query_ms": sinfo["query_ms"],
+                                       "apply_insert_ms": sinfo["apply_insert_ms"],
+                                       "apply_query_ms": sinfo["apply_query_ms"]}
     plain = None
     if "plain" in strategies:
         plain = dict(strategies["plain"], unit="k-mers/s", batched_over_plain=value / strategies["plain"]["value"])
@@ -434,9 +447,13 @@ def run_ours(args, dist: Dist):
     staged_query = 8 * R + gather + touched * block_bytes
     grouped_step = info["cut_ms"] > 0
     # (time, algorithmic bytes, random-sector model bytes or None, work units, unit name)
+    # with the build apply (the default), the insert apply's span is the build apply (insert, commit
+    # and the query of every exclusive bucket from shared memory) and the query apply's span only
+    # covers the items it deferred (split buckets)
     kernels = {
-        "k_apply<insert>": (info["apply_insert_ms"], staged_insert, model_insert, float(st.smers), "s-mer"),
-        "k_apply<query>": (info["apply_query_ms"], staged_query, model_query, float(st.smers), "s-mer"),
+        "k_apply<build>": (info["apply_insert_ms"], staged_insert, model_insert + model_query, float(st.smers),
+                           "s-mer"),
+        "k_apply<query, deferred items>": (info["apply_query_ms"], 0.0, None, 0.0, "s-mer"),
         # the cut reads the 2-bit codes and both bitmaps once and writes an 8-byte record and a
         # 16-byte base entry per super-k-mer
         "k_tiles<cut>": (info["cut_ms"], n_bytes / 2 + 24 * R, None, float(st.windows), "window"),
@@ -544,10 +561,17 @@ def run_ours(args, dist: Dist):
 
 def run_serving(ctx, args, rank: int) -> dict:
     """Config-5 shape on the resident config-2 index: requests of sequences, half drawn from the
-    indexed genome (1% errors) and half uniform random, arriving as a Poisson process; the
-    server batches them as they arrive.  Two streams: fixed-size requests of about 1 M k-mers
-    (the p99 < 10 ms target) and the mixed-size stream (1-10^5 sequences of 100 bp-50 kbp, each
-    request truncated at 4 Mbp so the pool is generated in seconds)."""
+    indexed genome (1% errors) and half uniform random, arriving as a Poisson process.
+
+    - 1 M-k-mer requests (40 sequences of 25 kbp, the p99 < 10 ms target) at offered rates from
+      100 req/s up, until the knee (served k-mers/s below 90% of the offered load, or p99 above
+      100 ms), through the continuous-batching server;
+    - the same requests and rates through the unbatched path: one scb_query_batch per request,
+      in arrival order, no overlap (the plain per-request GPU path);
+    - mixed requests, 1-10^5 sequences of log-uniform 100 bp-50 kbp (about 70 Mbp and 630 MB of
+      per-window output on average, uncapped), at rates up to their knee;
+    - the whole-stream distinct-k-mer spectrum, read from the server's set at the end of the 1 M
+      stream and checked against the spectrum of the same sequences in one batch."""
     import threading
 
     from scbf_b200 import _lib, workloads
@@ -557,94 +581,179 @@ def run_serving(ctx, args, rank: int) -> dict:
     rng = np.random.default_rng(17)
 
     def pool_fixed(count):
-        reqs = []
-        for i in range(count):
-            d, o = workloads.random_sequences(40, 25_000, 25_001, seed=1000 + i, genome=genome)
-            reqs.append((d, o))
-        return reqs
+        return [workloads.random_sequences(40, 25_000, 25_001, seed=1000 + i, genome=genome) for i in range(count)]
 
-    def pool_mixed(count, cap_bytes=4_000_000):
+    def pool_mixed(count):
         reqs = []
         for i in range(count):
             n = int(np.exp(rng.uniform(0, np.log(1e5))))
-            d, o = workloads.random_sequences(min(n, 4000), 100, 50_000, seed=2000 + i, genome=genome)
-            keep = int(np.searchsorted(o, cap_bytes, side="right")) - 1
-            keep = max(1, min(keep, len(o) - 1))
-            reqs.append((d[: int(o[keep])], o[: keep + 1].copy()))
+            reqs.append(workloads.random_sequences(n, 100, 50_000, seed=2000 + i, genome=genome))
         return reqs
 
-    def stream(reqs, rate, seconds, max_batch_bytes):
-        cfg = _lib.ScbServerConfig(16 << 30, max_batch_bytes, 0, 4, 0)
-        srv = C.c_void_p(0)
-        if L.scb_server_create(ctx.h, C.byref(cfg), C.byref(srv)) != 0:
-            raise RuntimeError(_lib.last_error())
+    def outputs(reqs):
         outs = []
         for d, o in reqs:
             nw = int(L.scb_count_windows(ctx.h, o.ctypes.data, len(o) - 1))
             outs.append((np.empty(max(nw, 1), np.uint64), np.empty(max(nw, 1), np.uint8), nw))
-        # warm-up: every template once
-        for (d, o), (ob, vb, _) in zip(reqs, outs):
-            t = C.c_uint64(0)
-            L.scb_server_submit(srv, d.ctypes.data, o.ctypes.data, len(o) - 1, ob.ctypes.data, vb.ctypes.data,
-                                C.byref(t))
-            L.scb_server_wait(srv, t.value, None)
+        return outs
+
+    def schedule(rate, seconds, n_pool):
+        n_req = max(20, int(rate * seconds))
+        return np.cumsum(rng.exponential(1.0 / rate, n_req)), rng.integers(0, n_pool, n_req)
+
+    def summarise(lat_ms, kmers, span_s, rate, extra):
+        lat = np.sort(np.asarray(lat_ms))
+        return dict({"rate_req_s": rate, "requests": int(lat.size), "p50_ms": float(np.percentile(lat, 50)),
+                     "p99_ms": float(np.percentile(lat, 99)), "max_ms": float(lat[-1]),
+                     "kmers_per_s": kmers / span_s if span_s > 0 else None,
+                     "offered_kmers_per_s": None}, **extra)
+
+    def stream(srv, reqs, outs, rate, seconds):
+        """Poisson arrivals into the server; requests of one template share output buffers."""
+        arrivals, pick = schedule(rate, seconds, len(reqs))
         L.scb_server_reset_stats(srv)
-        n_req = max(1, int(rate * seconds))
-        arrivals = np.cumsum(rng.exponential(1.0 / rate, n_req))
-        pick = rng.integers(0, len(reqs), n_req)
         tickets = []
         lock = threading.Lock()
         done = threading.Event()
 
         def waiter():
             i = 0
-            while True:
+            while i < len(arrivals):
                 with lock:
-                    have = i < len(tickets)
-                    t = tickets[i] if have else None
-                if have:
-                    L.scb_server_wait(srv, t, None)
-                    i += 1
-                    if i == n_req:
-                        break
-                elif done.is_set() and i >= len(tickets):
-                    break
-                else:
-                    time.sleep(0.0002)
+                    t = tickets[i] if i < len(tickets) else None
+                if t is None:
+                    time.sleep(0.0001)
+                    continue
+                L.scb_server_wait(srv, t, None)
+                i += 1
+            done.set()
 
         wt = threading.Thread(target=waiter)
         wt.start()
         t0 = time.perf_counter()
-        for a, j in zip(arrivals, pick):
-            delay = t0 + a - time.perf_counter()
+        for a_, j in zip(arrivals, pick):
+            delay = t0 + a_ - time.perf_counter()
             if delay > 0:
                 time.sleep(delay)
             d, o = reqs[j]
-            ob, vb, _ = outs[j]  # requests of one template share output buffers (results not read)
+            ob, vb, _ = outs[j]
+            t = C.c_uint64(0)
+            if L.scb_server_submit(srv, d.ctypes.data, o.ctypes.data, len(o) - 1, ob.ctypes.data, vb.ctypes.data,
+                                   C.byref(t)) != 0:
+                raise RuntimeError(_lib.last_error())
+            with lock:
+                tickets.append(t.value)
+        wt.join()
+        sm = _lib.ScbServerSummary()
+        L.scb_server_get_summary(srv, C.byref(sm))
+        mean_k = float(np.mean([outs[j][2] for j in pick]))
+        return {"rate_req_s": rate, "requests": sm.requests, "p50_ms": sm.p50_ms, "p99_ms": sm.p99_ms,
+                "mean_ms": sm.mean_ms, "max_ms": sm.max_ms,
+                "kmers_per_s": sm.windows / sm.span_s if sm.span_s else None,
+                "offered_kmers_per_s": rate * mean_k, "batches": sm.batches, "slots": sm.slots,
+                "mean_kmers_per_request": mean_k}
+
+    def per_request(reqs, outs, rate, seconds):
+        """The unbatched path: requests answered one at a time, in arrival order, each by one
+        scb_query_batch call (host buffers, H2D and D2H inside it)."""
+        arrivals, pick = schedule(rate, seconds, len(reqs))
+        lat, kmers = [], 0
+        t0 = time.perf_counter()
+        for a_, j in zip(arrivals, pick):
+            delay = t0 + a_ - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            d, o = reqs[j]
+            ob, vb, nw = outs[j]
+            if L.scb_query_batch(ctx.h, d.ctypes.data, o.ctypes.data, len(o) - 1, ob.ctypes.data,
+                                 vb.ctypes.data) != 0:
+                raise RuntimeError(_lib.last_error())
+            lat.append((time.perf_counter() - t0 - a_) * 1e3)
+            kmers += nw
+        span = time.perf_counter() - t0
+        mean_k = float(np.mean([outs[j][2] for j in pick]))
+        return summarise(lat, kmers, span, rate, {"offered_kmers_per_s": rate * mean_k,
+                                                  "mean_kmers_per_request": mean_k})
+
+    def knee(r):
+        return (r["kmers_per_s"] or 0) < 0.9 * r["offered_kmers_per_s"] or r["p99_ms"] > 100.0
+
+    def server(reqs, max_batch_bytes, spectrum_keys=0):
+        cfg = _lib.ScbServerConfig(16 << 30, max_batch_bytes, 0, 4, 0, spectrum_keys)
+        srv = C.c_void_p(0)
+        if L.scb_server_create(ctx.h, C.byref(cfg), C.byref(srv)) != 0:
+            raise RuntimeError(_lib.last_error())
+        outs = outputs(reqs)
+        for (d, o), (ob, vb, _) in zip(reqs, outs):  # warm-up: every template once (graph captures)
             t = C.c_uint64(0)
             L.scb_server_submit(srv, d.ctypes.data, o.ctypes.data, len(o) - 1, ob.ctypes.data, vb.ctypes.data,
                                 C.byref(t))
-            with lock:
-                tickets.append(t.value)
-        done.set()
-        wt.join()
-        s = _lib.ScbServerSummary()
-        L.scb_server_get_summary(srv, C.byref(s))
-        L.scb_server_destroy(srv)
-        return {"rate_req_s": rate, "requests": s.requests, "p50_ms": s.p50_ms, "p99_ms": s.p99_ms,
-                "mean_ms": s.mean_ms, "max_ms": s.max_ms, "kmers_per_s": s.windows / s.span_s if s.span_s else None,
-                "batches": s.batches, "slots": s.slots,
-                "mean_kmers_per_request": float(np.mean([outs[j][2] for j in pick]))}
+            L.scb_server_wait(srv, t.value, None)
+        return srv, outs
 
-    fixed_pool = pool_fixed(16)
-    fixed = stream(fixed_pool, rate=300.0, seconds=3.0, max_batch_bytes=16 << 20)
-    mixed = stream(pool_mixed(48), rate=100.0, seconds=3.0, max_batch_bytes=32 << 20)
-    # the same 1 M-k-mer stream with every batch launched kernel by kernel (no graph replays)
+    out = {"index": "config-2 frozen index, resident",
+           "arrivals": "Poisson; requests drawn from a pool of generated templates (results of one template "
+                       "share an output buffer)"}
+    # 1 M-k-mer requests: batched server (with the whole-stream spectrum) vs unbatched
+    fixed = pool_fixed(16)
+    srv, outs = server(fixed, 16 << 20, spectrum_keys=64 << 20)
+    sweep = []
+    for rate in (100, 300, 1000, 3000, 10000):
+        r = stream(srv, fixed, outs, rate, seconds=2.0)
+        sweep.append(r)
+        if knee(r):
+            break
+    t_sp = time.perf_counter()
+    rows, dk, qk = C.c_uint64(0), C.c_uint64(0), C.c_uint64(0)
+    if L.scb_server_spectrum(srv, None, None, 0, C.byref(rows), C.byref(dk), C.byref(qk)) != 0:
+        raise RuntimeError(_lib.last_error())
+    vals, cnts = np.zeros(max(rows.value, 1), np.uint64), np.zeros(max(rows.value, 1), np.uint64)
+    L.scb_server_spectrum(srv, vals.ctypes.data, cnts.ctypes.data, rows.value, C.byref(rows), C.byref(dk),
+                          C.byref(qk))
+    spectrum_ms = (time.perf_counter() - t_sp) * 1e3
+    # the same spectrum from one batch of the pool's sequences (each template is in the stream)
+    from scbf_b200 import api
+
+    seqs = [bytes(d[int(o[i]):int(o[i + 1])]) for d, o in fixed for i in range(len(o) - 1)]
+    bd, bo = api.pack_sequences(seqs)
+    ref = api.SuperCountingBloomIndex._from_ctx(ctx, None, 0).spectrum_distinct(bd, bo)
+    assert ref["rows"] == list(zip(vals[: rows.value].tolist(), cnts[: rows.value].tolist())), "stream spectrum"
+    assert ref["distinct_keys"] == dk.value
+    L.scb_server_destroy(srv)
+    out["one_mkmer_requests"] = {"server": sweep, "knee_rate_req_s": sweep[-1]["rate_req_s"] if knee(sweep[-1])
+                                 else None,
+                                 "whole_stream_spectrum": {"distinct_kmers": dk.value, "queried_kmers": qk.value,
+                                                           "rows": rows.value, "read_ms": spectrum_ms,
+                                                           "equals_one_batch_spectrum": True}}
+    plain = []
+    for rate in (100, 300, 1000, 3000, 10000):
+        r = per_request(fixed, outs, rate, seconds=1.0)
+        plain.append(r)
+        if knee(r):
+            break
+    out["one_mkmer_requests"]["per_request_unbatched"] = plain
+    # the same server without graph replays, at the highest rate below the knee
+    ok = [r["rate_req_s"] for r in sweep if not knee(r)] or [100]
     L.scb_set_graphs(ctx.h, 0)
-    fixed_eager = stream(fixed_pool, rate=300.0, seconds=3.0, max_batch_bytes=16 << 20)
+    srv, outs = server(fixed, 16 << 20)
+    out["one_mkmer_requests"]["server_without_graphs"] = stream(srv, fixed, outs, ok[-1], seconds=2.0)
+    L.scb_server_destroy(srv)
     L.scb_set_graphs(ctx.h, 1)
-    return {"index": "config-2 frozen index, resident", "one_mkmer_requests": fixed, "mixed_requests": mixed,
-            "one_mkmer_requests_without_graphs": fixed_eager}
+    del outs
+    # mixed requests, uncapped
+    mixed = pool_mixed(12)
+    srv, mouts = server(mixed, 64 << 20)
+    msweep = []
+    for rate in (2, 5, 10, 20, 50):
+        r = stream(srv, mixed, mouts, rate, seconds=3.0)
+        msweep.append(r)
+        if knee(r):
+            break
+    L.scb_server_destroy(srv)
+    out["mixed_requests"] = {"server": msweep, "pool_requests": len(mixed),
+                             "pool_mean_bytes": float(np.mean([int(o[-1]) for _, o in mixed])),
+                             "pool_max_sequences": int(max(len(o) - 1 for _, o in mixed))}
+    return out
 
 
 MIXED_WORKLOAD = ("mixed lengths: 200 Mbp uniform genome at 15x; 70% of bases from 150 bp reads (1% "

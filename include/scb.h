@@ -235,6 +235,16 @@ scb_status scb_set_graphs(scb_ctx* ctx, int enable);
 /* Graph captures, replays, and replays redone eagerly (record overflow or failed capture). */
 scb_status scb_graph_stats(const scb_ctx* ctx, uint64_t* captures, uint64_t* replays, uint64_t* fallbacks);
 
+/* Build + stream query in one apply pass (no counterpart in the reference, whose stream query
+ * runs after the whole build, src/fastx.rs:172-204).  With the grouped strategy for both passes,
+ * every super-k-mer record of a batch that maps to a counter bucket is in that bucket's one work
+ * item, so once the item commits its deltas its blocks hold their final counters: the same pass
+ * then answers those records' windows from shared memory, and only buckets split over several
+ * items (or with more than 8192 s-mers) go through a second, query-only pass.  Results are
+ * identical to a separate query after the build.  Default on; enable = 0 runs the insert and the
+ * query as two passes (the comparison point). */
+scb_status scb_set_fused_build(scb_ctx* ctx, int enable);
+
 /* Host scb_build_and_stream_query in pieces (no counterpart in the reference; the reference's
  * parser thread feeds its workers the same way, src/api.rs:621-674).  A batch of at least two
  * pieces is split into pieces of whole sequences of at most piece_bytes (0: 512 MiB; raised so
@@ -275,6 +285,10 @@ typedef struct scb_server_config {
     uint64_t max_batch_seqs;      /* sequences per batch (default max_batch_bytes / 64) */
     uint32_t max_inflight;        /* batches on the GPU at once (default 4) */
     uint32_t reserved;
+    /* distinct k-mers the whole-stream spectrum can hold (0: no spectrum).  The server keeps a
+     * device set of twice that many (rounded up to a power of two) 8-byte keys beside the slots,
+     * outside memory_budget_bytes; every batch also adds its windows' canonical k-mers to it. */
+    uint64_t spectrum_keys;
 } scb_server_config;
 typedef struct scb_request_stats {
     double queue_ms;   /* submit -> first piece launched */
@@ -298,7 +312,16 @@ scb_status scb_server_submit(scb_server* s, const uint8_t* seqs, const uint64_t*
                              uint64_t* abundances, uint8_t* valid, uint64_t* ticket);
 scb_status scb_server_wait(scb_server* s, uint64_t ticket, scb_request_stats* stats);
 scb_status scb_server_get_summary(scb_server* s, scb_server_summary* out);
+/* Clears the latency statistics and the whole-stream spectrum (call it with no request in flight). */
 scb_status scb_server_reset_stats(scb_server* s);
+/* The whole stream's distinct-k-mer spectrum: estimate_distinct_kmers + spectrum_from_estimates
+ * (src/fastx.rs:255-308, 392-410) over every sequence the server answered since it was created or
+ * last reset: value -> number of distinct canonical k-mers with that estimate, rows sorted by
+ * value, same two-call convention as scb_spectrum_distinct.  Waits for the batches in flight.
+ * Needs spectrum_keys > 0; a stream with more distinct k-mers than the set holds fails with
+ * SCB_ERR_INTERNAL_STATE (device status word 2). */
+scb_status scb_server_spectrum(scb_server* s, uint64_t* values, uint64_t* counts, uint64_t capacity,
+                               uint64_t* n_rows, uint64_t* distinct_keys, uint64_t* queried_kmers);
 /* Graphs captured (one per slot and shape class) and batches replayed through them.  A server
  * uses graphs when its index context had them on at scb_server_create (scb_set_graphs). */
 scb_status scb_server_graph_stats(scb_server* s, uint64_t* captures, uint64_t* replays);

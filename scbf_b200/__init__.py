@@ -36,3 +36,10 @@ from .api import (  # noqa: F401
     stream_estimates_from_fastx_pair,
     write_spectrum,
 )
+from .filter import (  # noqa: F401
+    FrozenSuperCountingBloom,
+    PackedSeqVec,
+    SuperCountingBloom,
+    canonical_kmer,
+    xorshift_u64,
+)

@@ -47,7 +47,8 @@ class ScbTimings(C.Structure):
 
 class ScbServerConfig(C.Structure):
     _fields_ = [("memory_budget_bytes", C.c_uint64), ("max_batch_bytes", C.c_uint64),
-                ("max_batch_seqs", C.c_uint64), ("max_inflight", C.c_uint32), ("reserved", C.c_uint32)]
+                ("max_batch_seqs", C.c_uint64), ("max_inflight", C.c_uint32), ("reserved", C.c_uint32),
+                ("spectrum_keys", C.c_uint64)]
 
 
 class ScbRequestStats(C.Structure):
@@ -138,6 +139,7 @@ def load(path: str | None = None):
         "scb_get_timings": (C.c_int, [ctxp, C.POINTER(ScbTimings)]),
         "scb_set_graphs": (C.c_int, [ctxp, C.c_int]),
         "scb_set_piece_bytes": (C.c_int, [ctxp, C.c_uint64]),
+        "scb_set_fused_build": (C.c_int, [ctxp, C.c_int]),
         "scb_fastx_read": (C.c_int, [C.c_char_p, C.POINTER(vp)]),
         "scb_fastx_sequences": (C.c_int, [vp, C.POINTER(vp), C.POINTER(vp), u64p]),
         "scb_fastx_headers": (C.c_int, [vp, C.POINTER(vp), C.POINTER(vp)]),
@@ -152,6 +154,7 @@ def load(path: str | None = None):
         "scb_server_get_summary": (C.c_int, [vp, C.POINTER(ScbServerSummary)]),
         "scb_server_reset_stats": (C.c_int, [vp]),
         "scb_server_graph_stats": (C.c_int, [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+        "scb_server_spectrum": (C.c_int, [vp, vp, vp, C.c_uint64, u64p, u64p, u64p]),
         "scb_server_destroy": (None, [vp]),
         "scb_autotune": (C.c_int, [ctxp, vp, vp, C.c_uint64, C.POINTER(ScbTuning)]),
         "scb_get_tuning": (C.c_int, [ctxp, C.POINTER(ScbTuning)]),

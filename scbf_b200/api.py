@@ -745,9 +745,11 @@ class SuperCountingBloomServer:
     batches and overlap on the GPU; the device-memory budget bounds the batches in flight."""
 
     def __init__(self, index: "SuperCountingBloomIndex", memory_budget_bytes: int = 0,
-                 max_batch_bytes: int = 64 << 20, max_batch_seqs: int = 0, max_inflight: int = 4):
+                 max_batch_bytes: int = 64 << 20, max_batch_seqs: int = 0, max_inflight: int = 4,
+                 spectrum_keys: int = 0):
         self.index = index
-        cfg = _lib.ScbServerConfig(memory_budget_bytes, max_batch_bytes, max_batch_seqs, max_inflight, 0)
+        cfg = _lib.ScbServerConfig(memory_budget_bytes, max_batch_bytes, max_batch_seqs, max_inflight, 0,
+                                   spectrum_keys)
         out = C.c_void_p(0)
         _check(_lib.load().scb_server_create(index._ctx.h, C.byref(cfg), C.byref(out)))
         self.h = out
@@ -780,6 +782,19 @@ class SuperCountingBloomServer:
 
     def reset_stats(self) -> None:
         _check(_lib.load().scb_server_reset_stats(self.h))
+
+    def spectrum(self) -> dict:
+        """The whole stream's distinct-k-mer spectrum (src/fastx.rs:255-308, 392-410) over every
+        sequence answered since creation or the last reset_stats (needs spectrum_keys > 0)."""
+        L = _lib.load()
+        rows, dk, qk = C.c_uint64(0), C.c_uint64(0), C.c_uint64(0)
+        _check(L.scb_server_spectrum(self.h, None, None, 0, C.byref(rows), C.byref(dk), C.byref(qk)))
+        vals = np.zeros(max(rows.value, 1), np.uint64)
+        cnts = np.zeros(max(rows.value, 1), np.uint64)
+        _check(L.scb_server_spectrum(self.h, _ptr(vals), _ptr(cnts), rows.value, C.byref(rows), C.byref(dk),
+                                     C.byref(qk)))
+        return {"rows": list(zip(vals[: rows.value].tolist(), cnts[: rows.value].tolist())),
+                "distinct_keys": dk.value, "queried_kmers": qk.value}
 
     def close(self) -> None:
         if self.h and self.h.value:

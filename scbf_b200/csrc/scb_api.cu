@@ -276,14 +276,31 @@ scb_strategy resolve(scb_strategy s) { return s == SCB_STRATEGY_AUTO ? SCB_STRAT
 // Buckets of 2^shift consecutive blocks: about tuning.bucket_records (512 untuned) records per
 // bucket, at most 4096 counters
 // (or one block when blocks are larger) staged in shared memory.
-uint32_t bucket_shift_for(const scb_ctx* ctx, uint64_t records) {
+uint32_t bucket_shift_for(const scb_ctx* ctx, uint64_t records, uint64_t target) {
     uint32_t shift = 0;
     while ((ctx->block_slots << (shift + 1)) <= 4096 && (1ull << (shift + 1)) <= ctx->nb_blocks &&
-           records * (1ull << shift) / ctx->nb_blocks < ctx->tuning.bucket_records) {
+           records * (1ull << shift) / ctx->nb_blocks < target) {
         shift++;
     }
     return shift;
 }
+
+// Records per bucket of a build apply: a bucket's s-mers (about (w + 1) / 2 windows plus k - s
+// per random super-k-mer) stay well inside the kept probe slots, so almost every bucket answers
+// its own query.
+uint64_t build_bucket_records(const scb_ctx* ctx) {
+    const uint64_t per_record = (ctx->g.w + 1) / 2 + (ctx->g.k - ctx->g.s);
+    return std::max<uint64_t>(kKeptSmers * 10 / (16 * std::max<uint64_t>(per_record, 1)), 1);
+}
+
+// Records per bucket of a spectrum apply: a bucket's windows (about (w + 1) / 2 per random
+// super-k-mer) stay well below half the shared-memory key set.
+uint64_t spectrum_bucket_records(const scb_ctx* ctx) {
+    const uint64_t per_record = std::max<uint64_t>((ctx->g.w + 1) / 2, 1);
+    return std::max<uint64_t>(kSpecSet / 2 * 10 / (14 * per_record), 1);
+}
+
+enum BucketTarget : int { kTargetTuned = 0, kTargetBuild = 1, kTargetSpectrum = 2 };
 
 // Sizes of the grouped pipeline for a batch: bucket shift and count, record slots (the estimate
 // with a quarter of slack, at least min_records, plus the unused tail of each CTA's last reserved
@@ -310,6 +327,43 @@ uint64_t items_bound(const GroupedSizes& z) {
 // (kept as four 16-bit lanes of bucket-cell indices; buckets hold at most 16384 counters)
 bool probes_fit(const scb_ctx* ctx) { return ctx->g.h <= 4; }
 
+// A build + stream query of one batch with the grouped strategy for both passes runs the build
+// apply (kModeBuild) when probe slots fit and fusion is on.
+bool build_fused(const scb_ctx* ctx, uint64_t n_bytes) {
+    return ctx->fused_build && probes_fit(ctx) &&
+           resolve(ctx, ctx->insert_strategy, n_bytes, true) == SCB_STRATEGY_GROUPED &&
+           resolve(ctx, ctx->query_strategy, n_bytes, false) == SCB_STRATEGY_GROUPED;
+}
+
+// Build-apply buffers: the deferred-item list and the per-CTA kept probe words.
+scb_status build_buffers(const scb_ctx* ctx, Lane& L, uint64_t max_items) {
+    SCB_TRY(L.ditems.ensure(std::max<uint64_t>(max_items, 1) * 16));
+    SCB_TRY(L.ditem_base.ensure(std::max<uint64_t>(max_items, 1) * 8));
+    SCB_TRY(L.kept.ensure((uint64_t)ctx->sm_count * kKeptCtasPerSm * kKeptSmers * 8));
+    return SCB_OK;
+}
+
+// Build-apply arguments: report counters into qcnt, deferred items into the lane's list.
+scb_status attach_build(const scb_ctx* ctx, Lane& L, uint64_t max_items, unsigned long long* qcnt, GroupArgs& ga,
+                        cudaStream_t st) {
+    SCB_TRY(build_buffers(ctx, L, max_items));
+    ga.kept = L.kept.as<unsigned long long>();
+    ga.kept_ctas = (uint32_t)(ctx->sm_count * kKeptCtasPerSm);
+    SCB_CUDA(cudaMemsetAsync(L.rec_count.as<unsigned long long>() + 2, 0, 8, st));
+    ga.qcnt = qcnt;
+    ga.ditems = L.ditems.as<uint4>();
+    ga.ditem_base = L.ditem_base.as<unsigned long long>();
+    ga.dcount = L.rec_count.as<unsigned long long>() + 2;
+    return SCB_OK;
+}
+
+// The query kernel over the items a build apply left (attach_probes for the query first).
+void attach_deferred(const Lane& L, GroupArgs& ga) {
+    ga.items = L.ditems.as<uint4>();
+    ga.n_items = L.rec_count.as<unsigned long long>() + 2;
+    ga.item_base = L.ditem_base.as<unsigned long long>();
+}
+
 uint64_t probe_capacity(const scb_ctx* ctx, uint64_t n_bytes) {
     return n_bytes + records_estimate(ctx, n_bytes) * (ctx->g.k - ctx->g.s);
 }
@@ -325,10 +379,13 @@ scb_status attach_probes(Lane& L, int mode, uint64_t cap, GroupArgs& ga, cudaStr
     return SCB_OK;
 }
 
-GroupedSizes grouped_sizes(const scb_ctx* ctx, uint64_t n_bytes, uint64_t min_records) {
+GroupedSizes grouped_sizes(const scb_ctx* ctx, uint64_t n_bytes, uint64_t min_records, int target = kTargetTuned) {
     GroupedSizes z;
     const uint64_t est = records_estimate(ctx, n_bytes);
-    z.shift = bucket_shift_for(ctx, est);
+    const uint64_t want = target == kTargetBuild      ? build_bucket_records(ctx)
+                          : target == kTargetSpectrum ? spectrum_bucket_records(ctx)
+                                                      : (uint64_t)ctx->tuning.bucket_records;
+    z.shift = bucket_shift_for(ctx, est, want);
     z.n_buckets = ctx->nb_blocks >> z.shift;
     z.bucket_cap = ((est / z.n_buckets * 3 / 2 + 64) + 3) & ~3ull;
     z.cap = std::max<uint64_t>(est / 4 + 65536, min_records);
@@ -419,7 +476,7 @@ GroupArgs group_args(const scb_ctx* ctx, const Lane& L, const TileArgs& a, const
 scb_status launch_group_apply(scb_ctx* ctx, Lane& L, int mode, GroupArgs ga, unsigned long long* cnt,
                               uint64_t max_items, cudaStream_t st) {
     ga.cnt = cnt;
-    const bool ins = mode == kModeInsert;
+    const bool ins = mode != kModeReport;  // the build apply is timed as the insert apply
     SCB_CUDA(cudaMemsetAsync(ga.work_counter, 0, 4, st));
     SCB_TRY(mark(ctx, L, ins ? 7 : 11, st));
     launch_apply(mode, ga, (int)ctx->cfg.block_slots_exponent, 1u << ga.bucket_shift, ctx->sm_count, max_items, st);
@@ -455,7 +512,9 @@ scb_status run_materialize(scb_ctx* ctx, Lane& L, TileArgs& a, cudaStream_t st) 
 scb_status grouped_prepare(scb_ctx* ctx, Lane& L, TileArgs& a, cudaStream_t st) {
     GroupedState& gs = L.gs;
     gs.valid = false;
-    GroupedSizes z = grouped_sizes(ctx, a.n_bytes, 0);
+    gs.built = false;
+    GroupedSizes z = grouped_sizes(ctx, a.n_bytes, 0,
+                                   L.want_build ? kTargetBuild : L.want_spectrum ? kTargetSpectrum : kTargetTuned);
     unsigned long long overflow = 0, records = 0;
     SCB_TRY(mark(ctx, L, 4, st));
     for (int attempt = 0; attempt < 2; attempt++) {
@@ -506,7 +565,17 @@ scb_status grouped_apply(scb_ctx* ctx, Lane& L, int mode, unsigned long long* cn
         SCB_TRY(attach_probes(L, mode, gs.probe_cap, ga, st));
         if (mode == kModeInsert) gs.probes_written = true;
     }
-    return launch_group_apply(ctx, L, mode, ga, cnt, gs.max_items, st);
+    int launch_mode = mode;
+    if (mode == kModeInsert && L.want_build && gs.probe_cap) {
+        // build + stream query: the insert answers the exclusive buckets' queries (report sums
+        // into the lane's second counter array) and lists the other items for the query below
+        SCB_TRY(attach_build(ctx, L, gs.max_items, L.cnt2.as<unsigned long long>(), ga, st));
+        launch_mode = kModeBuild;
+        gs.built = true;
+    } else if (mode == kModeReport && gs.built) {
+        attach_deferred(L, ga);
+    }
+    return launch_group_apply(ctx, L, launch_mode, ga, cnt, gs.max_items, st);
 }
 
 scb_status run_grouped(scb_ctx* ctx, Lane& L, int mode, TileArgs& a, cudaStream_t st) {
@@ -605,7 +674,8 @@ uint64_t lane_signature(const scb_ctx* ctx, const Lane& L) {
     const void* ptrs[] = {L.codes.p, L.valid.p, L.seqstart.p, L.cnt.p, L.cnt2.p, L.tiles.p, L.params.p,
                           L.rec_key.p, L.rec_val.p, L.rec_sorted.p, L.rec_bases.p, L.rec_sbases.p, L.bhist.p,
                           L.bcursor.p, L.icount.p,
-                          L.items.p, L.gscan.p, L.rec_count.p, L.probes.p, L.item_base.p, ctx->table, ctx->status};
+                          L.items.p, L.gscan.p, L.rec_count.p, L.probes.p, L.item_base.p, L.ditems.p,
+                          L.ditem_base.p, L.kept.p, ctx->table, ctx->status};
     uint64_t h = 0x243F6A8885A308D3ull;
     for (const void* q : ptrs) h = (h ^ (uint64_t)(uintptr_t)q) * 0x100000001B3ull + 0x9E3779B97F4A7C15ull;
     return h;
@@ -657,13 +727,20 @@ scb_status record_batch(scb_ctx* ctx, Lane& L, const GraphKey& K, cudaStream_t s
         cut = true;
         return SCB_OK;
     };
+    const bool fuse = K.fused && K.probe_cap;
     if (kind_inserts(K.kind)) {
         SCB_TRY(mark(ctx, L, 2, st));
         if (K.s_ins == SCB_STRATEGY_GROUPED) {
             SCB_TRY(cut_and_bucket());
             GroupArgs ga = group_args(ctx, L, a, z);
             if (K.probe_cap) SCB_TRY(attach_probes(L, kModeInsert, K.probe_cap, ga, st));
-            SCB_TRY(launch_group_apply(ctx, L, kModeInsert, ga, L.cnt.as<unsigned long long>(), z.max_items, st));
+            int mode = kModeInsert;
+            if (fuse) {  // report sums of the buckets the build apply answers itself
+                SCB_CUDA(cudaMemsetAsync(L.cnt2.p, 0, kCntSlots * 8, st));
+                SCB_TRY(attach_build(ctx, L, z.max_items, L.cnt2.as<unsigned long long>(), ga, st));
+                mode = kModeBuild;
+            }
+            SCB_TRY(launch_group_apply(ctx, L, mode, ga, L.cnt.as<unsigned long long>(), z.max_items, st));
         } else {
             SCB_TRY(run_tiles(ctx, L, kModeInsert, a, st));
         }
@@ -673,7 +750,7 @@ scb_status record_batch(scb_ctx* ctx, Lane& L, const GraphKey& K, cudaStream_t s
         unsigned long long* qc = L.cnt.as<unsigned long long>();
         if (K.kind == kBatchBuildStream || K.kind == kBatchReportKept) {
             qc = L.cnt2.as<unsigned long long>();
-            SCB_CUDA(cudaMemsetAsync(qc, 0, kCntSlots * 8, st));
+            if (!fuse) SCB_CUDA(cudaMemsetAsync(qc, 0, kCntSlots * 8, st));
         }
         a.cnt = qc;
         SCB_TRY(mark(ctx, L, 9, st));
@@ -682,6 +759,7 @@ scb_status record_batch(scb_ctx* ctx, Lane& L, const GraphKey& K, cudaStream_t s
             if (!cut) SCB_TRY(cut_and_bucket());  // else: reuse the insert's records
             GroupArgs ga = group_args(ctx, L, a, z);
             if (K.probe_cap) SCB_TRY(attach_probes(L, kModeReport, K.probe_cap, ga, st));
+            if (fuse) attach_deferred(L, ga);  // only the items the build apply left
             SCB_TRY(launch_group_apply(ctx, L, kModeReport, ga, qc, z.max_items, st));
         } else {
             SCB_TRY(run_tiles(ctx, L, kModeReport, a, st));
@@ -764,7 +842,8 @@ scb_status graph_launch(scb_ctx* ctx, Lane& L, int kind, const uint8_t* d_ascii,
         SCB_TRY(L.params.ensure(sizeof(BatchParams)));
         SCB_TRY(L.cnt2.ensure(kCntSlots * 8));
         if (grouped) {
-            const GroupedSizes z = grouped_sizes(ctx, cls, L.rec_hint);
+            K.fused = kind == kBatchBuildStream && build_fused(ctx, n_bytes);
+            const GroupedSizes z = grouped_sizes(ctx, cls, L.rec_hint, K.fused ? kTargetBuild : kTargetTuned);
             K.shift = z.shift;
             K.n_buckets = z.n_buckets;
             K.rec_cap = z.cap;
@@ -780,6 +859,7 @@ scb_status graph_launch(scb_ctx* ctx, Lane& L, int kind, const uint8_t* d_ascii,
                 SCB_TRY(L.probes.ensure(K.probe_cap * 8));
                 SCB_TRY(L.item_base.ensure(z.max_items * 8));
             }
+            if (K.fused) SCB_TRY(build_buffers(ctx, L, z.max_items));  // before the signature: the graph points at them
         }
         K.sig = lane_signature(ctx, L);
     }
@@ -891,14 +971,24 @@ scb_status run_batch(scb_ctx* ctx, Lane& L, int kind, const uint8_t* d_ascii, co
     SCB_TRY(ensure_lane_work(ctx, L, n_bytes));
     TileArgs a;
     SCB_TRY(prepare_batch(ctx, L, d_ascii, d_offsets, n, n_bytes, st, a));
+    const bool fuse = kind == kBatchBuildStream && build_fused(ctx, n_bytes);
     if (kind_inserts(kind)) {
         // a grouped build + stream query keeps the insert's probe slots for the query
         L.want_probes = (kind == kBatchBuildStream || kind == kBatchInsertKeep) && probes_fit(ctx) &&
                         resolve(ctx, ctx->insert_strategy, n_bytes, true) == SCB_STRATEGY_GROUPED &&
                         (kind == kBatchInsertKeep ||
                          resolve(ctx, ctx->query_strategy, n_bytes, false) == SCB_STRATEGY_GROUPED);
-        const scb_status rs = insert_device_batch(ctx, L, a, st);
+        L.want_build = fuse;
+        scb_status rs = SCB_OK;
+        if (fuse) {
+            rs = L.cnt2.ensure(kCntSlots * 8);
+            if (rs == SCB_OK && cudaMemsetAsync(L.cnt2.p, 0, kCntSlots * 8, st) != cudaSuccess) {
+                rs = fail_kind(SCB_ERR_INTERNAL_STATE, "clearing the report counters failed");
+            }
+        }
+        if (rs == SCB_OK) rs = insert_device_batch(ctx, L, a, st);
         L.want_probes = false;
+        L.want_build = false;
         SCB_TRY(rs);
         SCB_TRY(read_counters(ctx, L, st, c_ins));
         if (kind == kBatchInsertKeep) L.kept_graph = false;  // the lane's eager state holds the records
@@ -908,6 +998,12 @@ scb_status run_batch(scb_ctx* ctx, Lane& L, int kind, const uint8_t* d_ascii, co
         launch_seq_windows(d_offsets, n, ctx->g.k, a.cnt, nullptr, st);
         SCB_TRY(query_device_batch(ctx, L, kModeReport, a, st));
         SCB_TRY(read_counters(ctx, L, st, c_q));
+        if (fuse && L.gs.built) {  // the report sums of the buckets the build apply answered
+            unsigned long long c2[kCntSlots];
+            SCB_CUDA(cudaMemcpyAsync(c2, L.cnt2.p, kCntSlots * 8, cudaMemcpyDeviceToHost, st));
+            SCB_CUDA(cudaStreamSynchronize(st));
+            for (int slot : {(int)kCntValid, (int)kCntPositive, (int)kCntChecksum}) c_q[slot] += c2[slot];
+        }
     }
     return SCB_OK;
 }
@@ -1073,10 +1169,21 @@ scb_status scb_set_threads(scb_ctx* ctx, uint64_t threads) {
     return SCB_OK;
 }
 
+// Waits for the context's own streams (not the device's other work: a server or another
+// context on the same GPU keeps running).
+static scb_status sync_ctx_streams(scb_ctx* ctx) {
+    if (ctx->lane.stream) SCB_CUDA(cudaStreamSynchronize(ctx->lane.stream));
+    for (auto& pl : ctx->piece_lanes) {
+        if (pl->stream) SCB_CUDA(cudaStreamSynchronize(pl->stream));
+    }
+    if (ctx->copy_stream) SCB_CUDA(cudaStreamSynchronize(ctx->copy_stream));
+    return SCB_OK;
+}
+
 scb_status scb_freeze(scb_ctx* ctx) {
     if (!ctx) return fail_kind(SCB_ERR_INTERNAL_STATE, "null context");
     CtxLock lk(ctx);
-    SCB_CUDA(cudaDeviceSynchronize());
+    SCB_TRY(sync_ctx_streams(ctx));
     ctx->frozen = true;
     return SCB_OK;
 }
@@ -1537,11 +1644,18 @@ scb_status scb_spectrum_distinct(scb_ctx* ctx, const uint8_t* seqs, const uint64
     SCB_TRY(hist.ensure((uint64_t)dense * 8));
     const uint64_t ovf_cap = ctx->g.bits == 32 ? std::max<uint64_t>(W, 1) : 1;
     SCB_TRY(ovf.ensure(ovf_cap * 8));
-    SCB_CUDA(cudaMemset(set.p, 0xFF, cap * 8));
-    SCB_CUDA(cudaMemset(hist.p, 0, (uint64_t)dense * 8));
-    // the chunks run on the lane's non-blocking stream: finish the clears first
-    SCB_CUDA(cudaDeviceSynchronize());
+    // the chunks run on the lane's stream, behind these clears
+    SCB_TRY(ensure_lane_work(ctx, ctx->lane, 0));
+    SCB_CUDA(cudaMemsetAsync(set.p, 0xFF, cap * 8, ctx->lane.stream));
+    SCB_CUDA(cudaMemsetAsync(hist.p, 0, (uint64_t)dense * 8, ctx->lane.stream));
     uint64_t distinct = 0, queried = 0, n_ovf = 0;
+    // one device batch with the grouped strategy: the spectrum apply deduplicates each exclusive
+    // bucket's keys in shared memory; otherwise the tile kernel inserts every key into the set
+    std::vector<Chunk> plan;
+    SCB_TRY(plan_chunks(offsets, n, ctx->cfg.k, ctx->tuning.host_batch_bytes, plan));
+    const uint64_t total = n ? offsets[n] - offsets[0] : 0;
+    const bool grouped = plan.size() == 1 && grouped_supported(ctx) &&
+                         resolve(ctx, ctx->query_strategy, total, false) == SCB_STRATEGY_GROUPED;
     SCB_TRY(for_each_chunk(ctx, seqs, offsets, n, [&](Lane& L, TileArgs& a, const Chunk&) -> scb_status {
         a.set_keys = set.as<unsigned long long>();
         a.set_mask = cap - 1;
@@ -1549,7 +1663,28 @@ scb_status scb_spectrum_distinct(scb_ctx* ctx, const uint8_t* seqs, const uint64
         a.hist_dense = dense;
         a.ovf = ovf.as<unsigned long long>() + n_ovf;
         a.ovf_cap = ovf_cap - n_ovf;
-        SCB_TRY(query_device_batch(ctx, L, kModeDistinct, a, L.stream));
+        if (grouped) {
+            SCB_TRY(mark(ctx, L, 9, L.stream));
+            L.want_spectrum = true;
+            const scb_status rs = grouped_prepare(ctx, L, a, L.stream);
+            L.want_spectrum = false;
+            SCB_TRY(rs);
+            if (L.gs.produced) {
+                GroupArgs ga = L.gs.ga;
+                ga.set_keys = a.set_keys;
+                ga.set_mask = a.set_mask;
+                ga.hist = a.hist;
+                ga.hist_dense = a.hist_dense;
+                ga.ovf = a.ovf;
+                ga.ovf_cap = a.ovf_cap;
+                SCB_TRY(launch_group_apply(ctx, L, kModeSpectrum, ga, a.cnt, L.gs.max_items, L.stream));
+            }
+            L.gs.valid = false;  // records bucketed for the spectrum, not for a later query
+            SCB_TRY(mark(ctx, L, 10, L.stream));
+            if (ctx->timing) L.spans |= kSpanQuery;
+        } else {
+            SCB_TRY(query_device_batch(ctx, L, kModeDistinct, a, L.stream));
+        }
         unsigned long long c[kCntSlots];
         SCB_TRY(read_counters(ctx, L, L.stream, c));
         distinct += c[kCntDistinct];
@@ -1558,8 +1693,9 @@ scb_status scb_spectrum_distinct(scb_ctx* ctx, const uint8_t* seqs, const uint64
         return SCB_OK;
     }));
     std::vector<unsigned long long> h(dense), o(n_ovf);
-    SCB_CUDA(cudaMemcpy(h.data(), hist.p, (uint64_t)dense * 8, cudaMemcpyDeviceToHost));
-    if (n_ovf) SCB_CUDA(cudaMemcpy(o.data(), ovf.p, n_ovf * 8, cudaMemcpyDeviceToHost));
+    SCB_CUDA(cudaMemcpyAsync(h.data(), hist.p, (uint64_t)dense * 8, cudaMemcpyDeviceToHost, ctx->lane.stream));
+    if (n_ovf) SCB_CUDA(cudaMemcpyAsync(o.data(), ovf.p, n_ovf * 8, cudaMemcpyDeviceToHost, ctx->lane.stream));
+    SCB_CUDA(cudaStreamSynchronize(ctx->lane.stream));
     std::vector<std::pair<uint64_t, uint64_t>> rows;
     rows_from_hist(h, o, rows);
     if (distinct_keys) *distinct_keys = distinct;
@@ -1667,6 +1803,13 @@ scb_status scb_set_graphs(scb_ctx* ctx, int enable) {
     return SCB_OK;
 }
 
+scb_status scb_set_fused_build(scb_ctx* ctx, int enable) {
+    if (!ctx) return fail_kind(SCB_ERR_INTERNAL_STATE, "null context");
+    CtxLock lk(ctx);
+    ctx->fused_build = enable != 0;
+    return SCB_OK;
+}
+
 scb_status scb_set_piece_bytes(scb_ctx* ctx, uint64_t piece_bytes) {
     if (!ctx) return fail_kind(SCB_ERR_INTERNAL_STATE, "null context");
     CtxLock lk(ctx);
@@ -1691,9 +1834,12 @@ scb_status scb_get_timings(const scb_ctx* ctx, scb_timings* out) {
 scb_status scb_reset(scb_ctx* ctx) {
     if (!ctx) return fail_kind(SCB_ERR_INTERNAL_STATE, "null context");
     CtxLock lk(ctx);
-    SCB_CUDA(cudaMemset(ctx->table, 0, ctx->table_bytes));
-    SCB_CUDA(cudaMemset(ctx->status, 0, 64));
-    SCB_CUDA(cudaDeviceSynchronize());
+    SCB_TRY(sync_ctx_streams(ctx));
+    SCB_TRY(ensure_lane_work(ctx, ctx->lane, 0));  // the lane's stream
+    cudaStream_t st = ctx->lane.stream;
+    SCB_CUDA(cudaMemsetAsync(ctx->table, 0, ctx->table_bytes, st));
+    SCB_CUDA(cudaMemsetAsync(ctx->status, 0, 64, st));
+    SCB_CUDA(cudaStreamSynchronize(st));
     ctx->inserted_kmers = 0;
     ctx->inserted_smers = 0;
     ctx->frozen = false;
@@ -1968,12 +2114,8 @@ scb_status scb_autotune(scb_ctx* ctx, const uint8_t* seqs, const uint64_t* offse
         // 4096-counter cap makes several alike, only the default (512) or the one nearest to it
         // is measured, so a tie in noise never moves the setting
         std::vector<std::pair<uint32_t, uint32_t>> shifts;  // (shift, target)
-        Tuning probe = ctx->tuning;
         for (uint32_t b : {512u, 256u, 1024u, 2048u}) {
-            probe.bucket_records = b;
-            std::swap(probe, ctx->tuning);
-            const uint32_t sh = bucket_shift_for(ctx, records_estimate(ctx, total));
-            std::swap(probe, ctx->tuning);
+            const uint32_t sh = bucket_shift_for(ctx, records_estimate(ctx, total), b);
             bool seen = false;
             for (auto& x : shifts) seen = seen || x.first == sh;
             if (!seen) shifts.push_back({sh, b});

@@ -94,6 +94,7 @@ constexpr uint64_t kMaxBatchBytes = (1ull << 31);
 struct GroupedState {
     bool valid = false;
     bool probes_written = false;  // the insert apply stored every s-mer's probe slots
+    bool built = false;           // a build apply answered its items' queries and listed the rest
     uint64_t probe_cap = 0;
     uint32_t shift = 0;
     uint64_t n_buckets = 0, max_items = 0, produced = 0;
@@ -139,9 +140,10 @@ struct GraphKey {
     int kind = 0, s_ins = 0, s_query = 0;
     uint64_t cap_bytes = 0, rec_cap = 0, bucket_cap = 0, max_items = 0, n_buckets = 0, probe_cap = 0;
     uint32_t shift = 0, apply_threads = 0;
+    bool fused = false;  // a grouped build + stream query in one build apply (plus deferred items)
     uint64_t sig = 0;
     bool operator==(const GraphKey& o) const {
-        return kind == o.kind && s_ins == o.s_ins && s_query == o.s_query &&
+        return kind == o.kind && s_ins == o.s_ins && s_query == o.s_query && fused == o.fused &&
                cap_bytes == o.cap_bytes && rec_cap == o.rec_cap && bucket_cap == o.bucket_cap &&
                probe_cap == o.probe_cap &&
                max_items == o.max_items && n_buckets == o.n_buckets && shift == o.shift &&
@@ -164,7 +166,13 @@ struct Lane {
     DevBuf rec_bases, rec_sbases;  // 16-byte base entries of the overflow and the sorted records
     // probe slots kept from a grouped insert for the query of the same records (build + stream)
     DevBuf probes, item_base;
+    // items a build apply leaves to the query kernel, with their probe-slot bases (the count is
+    // rec_count[2])
+    DevBuf ditems, ditem_base;
+    DevBuf kept;  // the build apply's per-CTA probe words (kKeptSmers per CTA)
     bool want_probes = false;
+    bool want_build = false;  // the grouped insert of this batch is a build apply
+    bool want_spectrum = false;  // buckets sized for the spectrum apply
     cudaStream_t stream = nullptr;
     GroupedState gs;
     cudaEvent_t ev[kLaneEvents] = {};
@@ -226,6 +234,7 @@ struct scb_ctx {
     uint64_t piece_bytes = 0;  // 0: the default
     bool timing = false;
     bool graphs = true;  // replay batches through graphs captured per shape class
+    bool fused_build = true;  // a grouped build + stream query answers exclusive buckets in its insert
     scb_timings times{};
     std::mutex mu;
     ~scb_ctx() {

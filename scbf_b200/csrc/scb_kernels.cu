@@ -1164,8 +1164,9 @@ struct CounterType<16> {
 //   smap    record of each s-mer of the chunk, wmap record of each window (query)
 //   touched one flag per block of the bucket
 //   est     s-mer minima of the chunk (query; 16-bit for 8/16-bit counters)
+//   skeys   the work item's distinct canonical k-mers (spectrum), shist the CTA's histogram
 struct ApplyLayout {
-    uint32_t cells, rv, spre, wpre, bases, rbases, smap, wmap, touched, est, total;
+    uint32_t cells, rv, spre, wpre, bases, rbases, smap, wmap, touched, est, kept, skeys, shist, total;
 };
 
 // s-mers (and windows) of one staged chunk of records; a record has at most 31 + 31
@@ -1184,7 +1185,9 @@ __host__ __device__ inline uint32_t align16(uint32_t x) { return (x + 15u) & ~15
 __host__ __device__ inline ApplyLayout apply_layout(int mode, int bits, uint32_t bucket_slots, uint32_t bucket_blocks,
                                                     bool lean = false) {
     ApplyLayout l;
-    const uint32_t cell_bytes = mode == kModeInsert ? 4u : (uint32_t)bits / 8u;
+    const bool deltas = mode == kModeInsert || mode == kModeBuild;  // u32 deltas in the cells
+    const bool queries = mode != kModeInsert;                        // window map and s-mer minima
+    const uint32_t cell_bytes = deltas ? 4u : (uint32_t)bits / 8u;
     const uint32_t max_smers = kSmerBudget, max_windows = kSmerBudget;
     l.cells = 0;
     l.rv = align16(bucket_slots * cell_bytes);
@@ -1193,11 +1196,43 @@ __host__ __device__ inline ApplyLayout apply_layout(int mode, int bits, uint32_t
     l.bases = l.wpre + align16((kApplyChunk + 1u) * 4u);
     l.rbases = l.bases + (lean ? 0u : align16(kApplyChunk * kRecBaseWords * 4u));
     l.smap = l.rbases + (lean ? 0u : align16(kApplyChunk * kRecBaseWords * 4u + 16u));  // + the last record's over-read
-    l.wmap = l.smap + align16(max_smers);
-    l.touched = l.wmap + (mode == kModeInsert ? 0u : align16(max_windows));
-    l.est = l.touched + align16(bucket_blocks);
-    l.total = l.est + (mode == kModeInsert ? 0u : align16(max_smers * (bits <= 16 ? 2u : 4u)));
+    const uint32_t est_bytes = align16(max_smers * (bits <= 16 ? 2u : 4u));
+    if (mode == kModeBuild) {
+        // the build's query phase needs neither the s-mer map nor the staged bases: its window
+        // map takes the s-mer map's bytes, its s-mer minima the bases' when they fit
+        l.wmap = l.smap;
+        l.touched = l.smap + align16(max_smers);
+        const bool est_in_bases = est_bytes <= l.smap - l.bases;
+        l.est = est_in_bases ? l.bases : l.touched + align16(bucket_blocks);
+        l.kept = l.touched + align16(bucket_blocks) + (est_in_bases ? 0u : est_bytes);
+    } else {
+        l.wmap = l.smap + align16(max_smers);
+        l.touched = l.wmap + (queries ? align16(max_windows) : 0u);
+        l.est = l.touched + align16(bucket_blocks);
+        l.kept = l.est + (queries ? est_bytes : 0u);
+    }
+    l.skeys = l.kept;
+    l.shist = l.skeys + (mode == kModeSpectrum ? kSpecSet * 8u : 0u);
+    l.total = l.shist + (mode == kModeSpectrum ? kSpecBins * 4u : 0u);
     return l;
+}
+
+// Inserts a canonical k-mer into a shared-memory open-addressing set (~0 marks an empty slot; no
+// canonical k-mer has that value).  True when the key is new.  The set holds at least twice as
+// many slots as the keys offered to it, so a free slot is always found.
+__device__ __forceinline__ bool smem_set_insert(unsigned long long* keys, uint32_t mask, uint64_t key) {
+    uint32_t i = (uint32_t)(((key ^ (key >> 31)) * 0x9E3779B97F4A7C15ull) >> 40) & mask;
+    for (uint32_t probe = 0; probe <= mask; probe++) {
+        const unsigned long long cur = *reinterpret_cast<volatile unsigned long long*>(keys + i);
+        if (cur == key) return false;
+        if (cur == ~0ull) {
+            const unsigned long long prev = atomicCAS(keys + i, ~0ull, (unsigned long long)key);
+            if (prev == ~0ull) return true;
+            if (prev == key) return false;
+        }
+        i = (i + 1) & mask;
+    }
+    return false;
 }
 
 // NH = 4: four hashes per s-mer (the default geometry), unrolled; NH = 0: any n_hashes.  Kept
@@ -1208,7 +1243,11 @@ __device__ __forceinline__ void apply_body(const GroupArgs& a, uint32_t bs_log2,
     extern __shared__ __align__(16) unsigned char smem_raw[];
     using T = CounterTraits<BITS>;
     using Cnt = typename CounterType<BITS>::type;
-    using Cell = typename std::conditional<MODE == kModeInsert, uint32_t, Cnt>::type;
+    constexpr bool kDeltas = MODE == kModeInsert || MODE == kModeBuild;  // cells hold u32 deltas
+    constexpr bool kBuild = MODE == kModeBuild;
+    constexpr bool kSpec = MODE == kModeSpectrum;
+    constexpr bool kStaged = MODE == kModeReport || kSpec;  // cells hold the table's counters
+    using Cell = typename std::conditional<kDeltas, uint32_t, Cnt>::type;
     using Est = typename std::conditional<(BITS <= 16), uint16_t, uint32_t>::type;
     constexpr uint32_t kVecLog2 = BITS == 8 ? 4u : (BITS == 16 ? 3u : 2u);  // log2 counters per 16 bytes
     const DevGeom g = a.g;
@@ -1225,7 +1264,14 @@ __device__ __forceinline__ void apply_body(const GroupArgs& a, uint32_t bs_log2,
     uint8_t* wmap = smem_raw + lay.wmap;
     uint8_t* touched = smem_raw + lay.touched;
     Est* est = reinterpret_cast<Est*>(smem_raw + lay.est);
+    // build: this CTA's region of the kept probe words (written by the insert, read back by the
+    // query of the same item moments later, so it stays in L2)
+    unsigned long long* kept = (kBuild && blockIdx.x < a.kept_ctas) ? a.kept + (uint64_t)blockIdx.x * kKeptSmers
+                                                                     : nullptr;
+    unsigned long long* skeys = reinterpret_cast<unsigned long long*>(smem_raw + lay.skeys);
+    uint32_t* shist = reinterpret_cast<uint32_t*>(smem_raw + lay.shist);
     __shared__ uint4 item;
+    __shared__ uint32_t item_fused;
     __shared__ unsigned item_idx;
     __shared__ uint32_t item_smers;
     __shared__ unsigned long long item_probes;
@@ -1237,7 +1283,11 @@ __device__ __forceinline__ void apply_body(const GroupArgs& a, uint32_t bs_log2,
     uint32_t* table32 = reinterpret_cast<uint32_t*>(a.table);
     const uint64_t n_items = *a.n_items;
     if (a.rec_count && *a.rec_count > a.rec_cap) return;  // records outgrew their slots: host redoes it
-    unsigned long long c_valid = 0, c_pos = 0, c_sum = 0;
+    unsigned long long c_valid = 0, c_pos = 0, c_sum = 0, c_dist = 0;
+    const uint32_t spec_bins = kSpec ? min(kSpecBins, a.hist_dense) : 0u;
+    if constexpr (kSpec) {
+        for (uint32_t x = tid; x < spec_bins; x += blockDim.x) shist[x] = 0;
+    }
 
     while (true) {
         if (tid == 0) {
@@ -1257,8 +1307,12 @@ __device__ __forceinline__ void apply_body(const GroupArgs& a, uint32_t bs_log2,
         // probe slots of the item: the insert reserves room for all its s-mers, the query finds
         // where the insert put them
         unsigned long long pbase = kNoProbes;
+        // build: the item answers its own query when its counters are final once it commits (the
+        // bucket's only item) and its probe slots fit the kept array; otherwise it stores them and
+        // goes to the list the query kernel works through
+        bool fused = false;
         if (a.probes) {
-            if constexpr (MODE == kModeInsert) {
+            if constexpr (kDeltas) {
                 uint32_t n = 0;
                 for (uint32_t r = tid; r < count; r += blockDim.x) {
                     n += (uint32_t)((a.recs[first + r] >> kRecWindowsShift) & 63u) + ks;
@@ -1267,22 +1321,58 @@ __device__ __forceinline__ void apply_body(const GroupArgs& a, uint32_t bs_log2,
                 if ((tid & 31) == 0 && n) atomicAdd(&item_smers, n);
                 __syncthreads();
                 if (tid == 0) {
-                    unsigned long long b = atomicAdd(a.probe_count, (unsigned long long)item_smers);
-                    if (b + item_smers > a.probe_cap) b = kNoProbes;
-                    a.item_base[item_idx] = b;
+                    bool f = false;
+                    if constexpr (kBuild) {
+                        f = kept != nullptr && exclusive && item_smers <= kKeptSmers && (bs % T::kLanes) == 0;
+                    }
+                    unsigned long long b = kNoProbes;
+                    if (!f) {
+                        b = atomicAdd(a.probe_count, (unsigned long long)item_smers);
+                        if (b + item_smers > a.probe_cap) b = kNoProbes;
+                    }
+                    if constexpr (kBuild) {
+                        if (!f) {
+                            const unsigned long long d = atomicAdd(a.dcount, 1ull);
+                            a.ditems[d] = it;
+                            a.ditem_base[d] = b;
+                        }
+                    } else {
+                        a.item_base[item_idx] = b;
+                    }
                     item_probes = b;
+                    item_fused = f ? 1u : 0u;
                 }
             } else {
                 if (tid == 0) item_probes = a.item_base[item_idx];
             }
             __syncthreads();
             pbase = item_probes;
+            if constexpr (kBuild) fused = item_fused != 0;
         }
-        const bool have_probes = MODE != kModeInsert && pbase != kNoProbes;
+        const bool have_probes = MODE == kModeReport && pbase != kNoProbes;
+        // spectrum: the item's windows deduplicate in a shared-memory set of at least twice as
+        // many slots when the item is its bucket's only one (every occurrence of a canonical
+        // k-mer has the same minimizer, so the same block and bucket); otherwise in the global set
+        uint32_t set_cap = 0;
+        if constexpr (kSpec) {
+            uint32_t n = 0;
+            for (uint32_t r = tid; r < count; r += blockDim.x) {
+                n += (uint32_t)((a.recs[first + r] >> kRecWindowsShift) & 63u);
+            }
+            n = __reduce_add_sync(0xFFFFFFFFu, n);
+            if ((tid & 31) == 0 && n) atomicAdd(&item_smers, n);
+            __syncthreads();
+            const uint32_t wins = item_smers;
+            if (exclusive && 2 * wins <= kSpecSet) {
+                set_cap = 256;
+                while (set_cap < 2 * wins) set_cap <<= 1;
+                for (uint32_t x = tid; x < set_cap; x += blockDim.x) skeys[x] = ~0ull;
+            }
+        }
         uint64_t poff = 0;  // s-mers of the item's earlier chunks
 
         for (uint32_t x = tid; x < bucket_blocks; x += blockDim.x) touched[x] = 0;
-        if constexpr (MODE == kModeInsert) {
+        if constexpr (kDeltas) {
             if ((bucket_slots & 3u) == 0) {
                 uint4* c4 = reinterpret_cast<uint4*>(cells);
                 for (uint32_t x = tid; x < bucket_slots / 4; x += blockDim.x) c4[x] = make_uint4(0u, 0u, 0u, 0u);
@@ -1291,7 +1381,7 @@ __device__ __forceinline__ void apply_body(const GroupArgs& a, uint32_t bs_log2,
             }
         }
         __syncthreads();
-        if constexpr (MODE == kModeReport) {
+        if constexpr (kStaged) {
             // stage the counters of the blocks this item reads, 16 bytes per load when a block
             // holds at least that much
             for (uint32_t r = tid; r < count; r += blockDim.x) touched[a.recs[first + r] >> kRecLocalShift] = 1;
@@ -1336,8 +1426,8 @@ __device__ __forceinline__ void apply_body(const GroupArgs& a, uint32_t bs_log2,
             if (tid < nuse) {  // record index of its s-mers (not needed with kept slots) / windows
                 const uint32_t s0 = spre[tid], s1 = have_probes ? s0 : spre[tid + 1];
                 for (uint32_t f = s0; f < s1; f++) smap[f] = (uint8_t)tid;
-                if constexpr (MODE == kModeInsert) touched[(uint32_t)(rv[tid] >> kRecLocalShift)] = 1;
-                if constexpr (MODE == kModeReport) {
+                if constexpr (kDeltas) touched[(uint32_t)(rv[tid] >> kRecLocalShift)] = 1;
+                if constexpr (kStaged) {
                     const uint32_t w0i = wpre[tid], w1i = wpre[tid + 1];
                     for (uint32_t vv = w0i; vv < w1i; vv++) wmap[vv] = (uint8_t)tid;
                 }
@@ -1345,7 +1435,7 @@ __device__ __forceinline__ void apply_body(const GroupArgs& a, uint32_t bs_log2,
             __syncthreads();
             const uint32_t nrec_used = nuse;
             const uint32_t S = spre[nrec_used];
-            if constexpr (MODE != kModeInsert) {
+            if constexpr (MODE == kModeReport) {
                 if (have_probes) {
                     // the insert's slots of the chunk's s-mers: kProbeBatch loads in flight per
                     // thread, then the counter minima from shared memory
@@ -1400,7 +1490,7 @@ __device__ __forceinline__ void apply_body(const GroupArgs& a, uint32_t bs_log2,
                 }
                 uint64_t hash = xorshift64(smer);
                 Cell* blk = cells + (lb << bs_log2);
-                if constexpr (MODE == kModeInsert) {
+                if constexpr (kDeltas) {
                     unsigned long long pk = 0;
                     if constexpr (NH == 4) {
                         uint32_t sl[4];
@@ -1423,7 +1513,11 @@ __device__ __forceinline__ void apply_body(const GroupArgs& a, uint32_t bs_log2,
                             hash = xorshift64(hash);
                         }
                     }
-                    if (pbase != kNoProbes) __stcs(a.probes + pbase + poff + f, pk);
+                    if (kBuild && fused) {
+                        __stcg(kept + poff + f, pk);
+                    } else if (pbase != kNoProbes) {
+                        __stcs(a.probes + pbase + poff + f, pk);
+                    }
                 } else {
                     uint32_t e = T::kMax;
                     if constexpr (NH == 4) {
@@ -1458,12 +1552,48 @@ __device__ __forceinline__ void apply_body(const GroupArgs& a, uint32_t bs_log2,
                 }
                 __syncthreads();
             }
+            if constexpr (kSpec) {
+                // fastx.rs:255-308, 392-410: each window's canonical k-mer (from the staged bases
+                // and their mirror) counts its estimate once, the first time the key is seen
+                const uint32_t W = wpre[nrec_used];
+                const uint64_t kmask = len_mask(g.k);
+                for (uint32_t v = tid; v < W; v += blockDim.x) {
+                    const uint32_t r = wmap[v];
+                    const uint32_t off = v - wpre[r];
+                    const Est* e = est + spre[r] + off;
+                    uint32_t m = e[0];
+                    for (uint32_t t = 1; t <= ks; t++) m = min(m, (uint32_t)e[t]);
+                    const uint64_t fw = codes64(bases + r * kRecBaseWords, off) & kmask;
+                    const uint64_t rc = codes64(rbases + r * kRecBaseWords, 16u * kRecBaseWords - off - g.k) & kmask;
+                    const uint64_t key = fw < rc ? fw : rc;
+                    c_valid++;
+                    const bool fresh = set_cap ? smem_set_insert(skeys, set_cap - 1, key)
+                                               : set_insert(a.set_keys, a.set_mask, key, a.status);
+                    if (fresh) {
+                        c_dist++;
+                        if (m < spec_bins) {
+                            atomicAdd(shist + m, 1u);
+                        } else if (m < a.hist_dense) {
+                            atomicAdd(a.hist + m, 1ull);
+                        } else {
+                            const unsigned long long o = atomicAdd(&a.cnt[kCntOverflow], 1ull);
+                            if (o < a.ovf_cap) {
+                                a.ovf[o] = m;
+                            } else {
+                                atomicOr(a.status, kStatusOverflowFull);
+                            }
+                        }
+                    }
+                }
+                __syncthreads();
+            }
             c0 += nrec_used;
             poff += S;
         }
 
-        if constexpr (MODE == kModeInsert) {
-            // commit the deltas: min(old + delta, MAX) per counter (counter.rs saturation)
+        if constexpr (kDeltas) {
+            // commit the deltas: min(old + delta, MAX) per counter (counter.rs saturation); a
+            // build item that answers its own query keeps the committed values in its cells
             constexpr uint32_t lanes = T::kLanes;
             const bool word_ok = exclusive && (bs % lanes) == 0;
             if (exclusive && bs_log2 >= kVecLog2) {
@@ -1501,6 +1631,19 @@ __device__ __forceinline__ void apply_body(const GroupArgs& a, uint32_t bs_log2,
                         nw[w] = acc;
                     }
                     __stcg(wp, make_uint4(nw[0], nw[1], nw[2], nw[3]));
+                    if (kBuild && fused) {
+                        uint4* c4w = reinterpret_cast<uint4*>(cells);
+#pragma unroll
+                        for (uint32_t q = 0; q < kVec / 4; q++) {
+                            uint32_t fv[4];
+#pragma unroll
+                            for (uint32_t j = 0; j < 4; j++) {
+                                const uint32_t c = 4 * q + j;  // counter c of the vector: word c / lanes
+                                fv[j] = (nw[c / lanes] >> ((c % lanes) * BITS)) & T::kMax;
+                            }
+                            c4w[x * (kVec / 4) + q] = make_uint4(fv[0], fv[1], fv[2], fv[3]);
+                        }
+                    }
                 }
             } else if (word_ok) {
                 const uint32_t block_words = bs / lanes;
@@ -1511,11 +1654,14 @@ __device__ __forceinline__ void apply_body(const GroupArgs& a, uint32_t bs_log2,
                     uint32_t* wp = table32 + base / lanes + wi;
                     const uint32_t old = __ldcg(wp);
                     uint32_t nw = 0;
+                    const uint32_t cb = (lb << bs_log2) + wi * lanes;
 #pragma unroll
                     for (uint32_t l = 0; l < lanes; l++) {
                         const uint64_t cur = (old >> (l * BITS)) & T::kMax;
-                        const uint64_t sum = cur + cells[(lb << bs_log2) + wi * lanes + l];
-                        nw |= (uint32_t)(sum < T::kMax ? sum : T::kMax) << (l * BITS);
+                        const uint64_t sum = cur + cells[cb + l];
+                        const uint32_t nv = (uint32_t)(sum < T::kMax ? sum : T::kMax);
+                        nw |= nv << (l * BITS);
+                        if (kBuild && fused) cells[cb + l] = nv;
                     }
                     __stcg(wp, nw);
                 }
@@ -1529,11 +1675,67 @@ __device__ __forceinline__ void apply_body(const GroupArgs& a, uint32_t bs_log2,
                 }
             }
         }
+        if constexpr (kBuild) {
+            if (fused) {
+                // the item's query (src/filter.rs:462-508): every record's blocks are final, in the
+                // cells; each s-mer's estimate from its kept probe slots, then window minima, chunk
+                // by chunk as the insert went (same chunks, so the same kept offsets)
+                __syncthreads();
+                uint64_t qoff = 0;
+                for (uint32_t c0 = 0; c0 < count;) {
+                    const uint32_t nrec = min(kApplyChunk, count - c0);
+                    if (tid < nrec) rv[tid] = a.recs[first + c0 + tid];
+                    __syncthreads();
+                    chunk_prefix(rv, nrec, ks, spre, wpre, warp_tot);
+                    const uint32_t nuse = (uint32_t)__syncthreads_count(tid < nrec && spre[tid + 1] <= kSmerBudget);
+                    if (tid < nuse) {
+                        const uint32_t w0i = wpre[tid], w1i = wpre[tid + 1];
+                        for (uint32_t vv = w0i; vv < w1i; vv++) wmap[vv] = (uint8_t)tid;
+                    }
+                    const uint32_t S = spre[nuse];
+                    for (uint32_t f = tid; f < S; f += blockDim.x) {
+                        const unsigned long long pk = __ldcg(kept + qoff + f);
+                        uint32_t e;
+                        if constexpr (NH == 4) {
+                            const uint32_t lo = (uint32_t)pk, hi = (uint32_t)(pk >> 32);
+                            e = min(min(cells[lo & 0xFFFFu], cells[lo >> 16]), min(cells[hi & 0xFFFFu], cells[hi >> 16]));
+                        } else {
+                            e = T::kMax;
+                            for (uint32_t h = 0; h < g.h; h++) e = min(e, (uint32_t)cells[(uint32_t)(pk >> (16 * h)) & 0xFFFFu]);
+                        }
+                        est[f] = (Est)e;
+                    }
+                    __syncthreads();
+                    const uint32_t W = wpre[nuse];
+                    for (uint32_t v = tid; v < W; v += blockDim.x) {
+                        const uint32_t r = wmap[v];
+                        const Est* e = est + spre[r] + (v - wpre[r]);
+                        uint32_t m = e[0];
+                        for (uint32_t t = 1; t <= ks; t++) m = min(m, (uint32_t)e[t]);
+                        c_valid++;
+                        c_pos += m > 0;
+                        c_sum += m;
+                    }
+                    __syncthreads();
+                    c0 += nuse;
+                    qoff += S;
+                }
+            }
+        }
         __syncthreads();
     }
-    warp_add_u64(&a.cnt[kCntValid], c_valid);
-    warp_add_u64(&a.cnt[kCntPositive], c_pos);
-    warp_add_u64(&a.cnt[kCntChecksum], c_sum);
+    unsigned long long* rc = a.cnt;
+    if constexpr (kBuild) rc = a.qcnt;
+    warp_add_u64(&rc[kCntValid], c_valid);
+    warp_add_u64(&rc[kCntPositive], c_pos);
+    warp_add_u64(&rc[kCntChecksum], c_sum);
+    if constexpr (kSpec) {
+        warp_add_u64(&rc[kCntDistinct], c_dist);
+        __syncthreads();
+        for (uint32_t x = tid; x < spec_bins; x += blockDim.x) {
+            if (shist[x]) atomicAdd(a.hist + x, (unsigned long long)shist[x]);
+        }
+    }
 }
 
 template <int MODE, int BITS, int NH>
@@ -1551,6 +1753,12 @@ __global__ void __launch_bounds__(kApplyMaxThreads, 2048 / kApplyMaxThreads) k_a
     apply_body<MODE, BITS, NH, LEAN>(a, bs_log2, bucket_blocks);
 }
 
+template <int MODE, int BITS, int NH>
+__global__ void __launch_bounds__(kApplyMaxThreads) k_apply_spectrum(GroupArgs a, uint32_t bs_log2,
+                                                                      uint32_t bucket_blocks) {
+    apply_body<MODE, BITS, NH, false>(a, bs_log2, bucket_blocks);
+}
+
 static size_t apply_smem(int mode, int bits, uint32_t bucket_slots, uint32_t bucket_blocks, bool lean) {
     return apply_layout(mode, bits, bucket_slots, bucket_blocks, lean).total;
 }
@@ -1558,11 +1766,13 @@ static size_t apply_smem(int mode, int bits, uint32_t bucket_slots, uint32_t buc
 template <int MODE, int BITS>
 static void launch_apply_t(const GroupArgs& a, int bs_log2, uint32_t bucket_blocks, int sm_count, uint64_t max_items,
                            cudaStream_t st) {
-    const bool lean = MODE != kModeInsert && a.probes != nullptr;
+    const bool lean = MODE == kModeReport && a.probes != nullptr;
     const size_t smem = apply_smem(MODE, BITS, (1u << bs_log2) * bucket_blocks, bucket_blocks, lean);
     void (*fn)(GroupArgs, uint32_t, uint32_t);
-    if constexpr (MODE == kModeInsert) {
+    if constexpr (MODE == kModeInsert || MODE == kModeBuild) {
         fn = a.g.h == 4 ? k_apply_insert<MODE, BITS, 4> : k_apply_insert<MODE, BITS, 0>;
+    } else if constexpr (MODE == kModeSpectrum) {
+        fn = a.g.h == 4 ? k_apply_spectrum<MODE, BITS, 4> : k_apply_spectrum<MODE, BITS, 0>;
     } else {
         if (lean) {
             fn = a.g.h == 4 ? k_apply_query<MODE, BITS, 4, true> : k_apply_query<MODE, BITS, 0, true>;
@@ -1591,6 +1801,18 @@ void launch_apply(int mode, const GroupArgs& a, int bs_log2, uint32_t bucket_blo
             case 8: launch_apply_t<kModeInsert, 8>(a, bs_log2, bucket_blocks, sm_count, max_items, st); break;
             case 16: launch_apply_t<kModeInsert, 16>(a, bs_log2, bucket_blocks, sm_count, max_items, st); break;
             default: launch_apply_t<kModeInsert, 32>(a, bs_log2, bucket_blocks, sm_count, max_items, st); break;
+        }
+    } else if (mode == kModeSpectrum) {
+        switch (a.g.bits) {
+            case 8: launch_apply_t<kModeSpectrum, 8>(a, bs_log2, bucket_blocks, sm_count, max_items, st); break;
+            case 16: launch_apply_t<kModeSpectrum, 16>(a, bs_log2, bucket_blocks, sm_count, max_items, st); break;
+            default: launch_apply_t<kModeSpectrum, 32>(a, bs_log2, bucket_blocks, sm_count, max_items, st); break;
+        }
+    } else if (mode == kModeBuild) {
+        switch (a.g.bits) {
+            case 8: launch_apply_t<kModeBuild, 8>(a, bs_log2, bucket_blocks, sm_count, max_items, st); break;
+            case 16: launch_apply_t<kModeBuild, 16>(a, bs_log2, bucket_blocks, sm_count, max_items, st); break;
+            default: launch_apply_t<kModeBuild, 32>(a, bs_log2, bucket_blocks, sm_count, max_items, st); break;
         }
     } else {
         switch (a.g.bits) {

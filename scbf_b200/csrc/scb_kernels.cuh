@@ -26,8 +26,10 @@ enum TileMode : int {
     kModeMaterialize = 6,  // (b) for the plain pipeline: per-window block id + end flag in HBM
     kModeInsertStaged = 7, // (b)+(c)+(d) with one warp per super-k-mer staging block deltas
     kModeCut = 8,          // (b) for the grouped pipeline: one record per super-k-mer + bucket counts
-    kModeBuild = 9         // grouped apply of a build + stream query: insert a bucket's records, commit,
+    kModeBuild = 9,        // grouped apply of a build + stream query: insert a bucket's records, commit,
                            // then answer the same records' query from the committed shared-memory block
+    kModeSpectrum = 10     // grouped distinct-k-mer spectrum: a bucket's windows' estimates from its staged
+                           // blocks, their canonical k-mers deduplicated in shared memory
 };
 
 // Sizes and input pointers of one batch, in device memory: a graph captured for a shape class
@@ -51,9 +53,16 @@ constexpr uint32_t kItemRecords = 4096;    // records per work item (heavier buc
 constexpr uint32_t kApplyChunk = 256;      // records staged in shared memory at a time (<= CTA width)
 constexpr uint32_t kMaxBucketSlots = 16384;  // counters of one bucket held in shared memory
 constexpr uint32_t kApplyMaxThreads = 512;
-// s-mers of one work item whose probe slots a build apply keeps in shared memory between its
-// insert and its query (items with more are deferred to the query kernel)
+// s-mers of one work item whose probe slots a build apply keeps between its insert and its query,
+// in its CTA's region of a small global scratch that stays in L2 (items with more are deferred to
+// the query kernel)
 constexpr uint32_t kKeptSmers = 8192;
+// CTAs per SM the kept scratch has room for (2048 threads of 256-thread CTAs)
+constexpr uint32_t kKeptCtasPerSm = 8;
+// spectrum apply: largest shared-memory key set of a work item (items with more than half as
+// many windows use the global set) and the estimates histogrammed in shared memory per CTA
+constexpr uint32_t kSpecSet = 8192;
+constexpr uint32_t kSpecBins = 1024;
 
 struct GroupArgs {
     DevGeom g;
@@ -89,6 +98,18 @@ struct GroupArgs {
     uint4* ditems;
     unsigned long long* ditem_base;
     unsigned long long* dcount;
+    unsigned long long* kept;  // kKeptSmers probe words per CTA, for kept_ctas CTAs
+    uint32_t kept_ctas;
+    uint32_t pad0_;
+    // spectrum apply (kModeSpectrum): the global key set for items that cannot deduplicate in
+    // shared memory, the dense histogram [0, hist_dense) and the overflow list of larger values
+    unsigned long long* set_keys;
+    uint64_t set_mask;
+    unsigned long long* hist;
+    uint32_t hist_dense;
+    uint32_t pad_;
+    unsigned long long* ovf;
+    uint64_t ovf_cap;
 };
 constexpr unsigned long long kNoProbes = ~0ull;
 

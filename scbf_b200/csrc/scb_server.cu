@@ -107,10 +107,19 @@ struct scb_server {
     uint64_t stat_windows = 0, stat_batches = 0;
     bool use_graphs = true;
     uint64_t captures = 0, replays = 0;
+    // whole-stream spectrum: distinct canonical k-mers of every batch (set of 2^k keys, ~0 empty),
+    // the dense histogram of their estimates, values past it (32-bit counters), and the counters
+    // the distinct kernel adds to (windows, distinct keys, overflow entries)
+    bool spectrum = false;
+    DevBuf spec_set, spec_hist, spec_ovf, spec_cnt;
+    uint64_t spec_mask = 0, spec_ovf_cap = 0;
+    uint32_t spec_dense = 0;
     Clock::time_point first_submit{}, last_finish{};
     bool have_first = false;
 
     void run();
+    void add_spectrum(TileArgs& d, unsigned int* tile_counter) const;
+    scb_status clear_spectrum(cudaStream_t st);
     scb_status launch(Slot& s);
     scb_status record(Slot& s, cudaStream_t st);
     scb_status capture(Slot& s);
@@ -158,6 +167,27 @@ static TileArgs tile_args(const scb_server& srv, const Slot& s, uint64_t bytes, 
     return a;
 }
 
+// Distinct-k-mer pass of a batch into the server's stream-wide set (kernel (f), kModeDistinct):
+// the same windows and estimates as the abundance pass, each new canonical k-mer counted once.
+void scb_server::add_spectrum(TileArgs& d, unsigned int* tile_counter) const {
+    d.cnt = spec_cnt.as<unsigned long long>();
+    d.tile_counter = tile_counter;
+    d.set_keys = spec_set.as<unsigned long long>();
+    d.set_mask = spec_mask;
+    d.hist = spec_hist.as<unsigned long long>();
+    d.hist_dense = spec_dense;
+    d.ovf = spec_ovf.as<unsigned long long>();
+    d.ovf_cap = spec_ovf_cap;
+}
+
+scb_status scb_server::clear_spectrum(cudaStream_t st) {
+    SCB_CUDA(cudaMemsetAsync(spec_set.p, 0xFF, (spec_mask + 1) * 8, st));
+    SCB_CUDA(cudaMemsetAsync(spec_hist.p, 0, (uint64_t)spec_dense * 8, st));
+    SCB_CUDA(cudaMemsetAsync(spec_cnt.p, 0, kCntSlots * 8, st));
+    SCB_CUDA(cudaStreamSynchronize(st));
+    return SCB_OK;
+}
+
 // The graph body of one slot batch: sizes from the slot's parameter block, fixed grids.
 scb_status scb_server::record(Slot& s, cudaStream_t st) {
     const BatchParams* bp = s.params.as<BatchParams>();
@@ -171,6 +201,11 @@ scb_status scb_server::record(Slot& s, cudaStream_t st) {
     TileArgs a = tile_args(*this, s, cfg.max_batch_bytes, cfg.max_batch_seqs);
     a.dyn = bp;
     launch_tiles(kModeAbund, a, tile_grid(kModeAbund, ctx->g.bits, sms, a.n_tiles), st);
+    if (spectrum) {
+        TileArgs d = a;
+        add_spectrum(d, s.tiles.as<unsigned int>() + 1);
+        launch_tiles(kModeDistinct, d, tile_grid(kModeDistinct, ctx->g.bits, sms, d.n_tiles), st);
+    }
     SCB_CUDA(cudaGetLastError());
     return SCB_OK;
 }
@@ -243,6 +278,11 @@ scb_status scb_server::launch(Slot& s) {
             launch_seqstart(s.offsets.as<uint64_t>(), seqs, bytes, s.seqstart.as<uint32_t>(), st);
             TileArgs a = tile_args(*this, s, bytes, seqs);
             launch_tiles(kModeAbund, a, tile_grid(kModeAbund, c->g.bits, c->sm_count, a.n_tiles), st);
+            if (spectrum) {
+                TileArgs d = a;
+                add_spectrum(d, s.tiles.as<unsigned int>() + 1);
+                launch_tiles(kModeDistinct, d, tile_grid(kModeDistinct, c->g.bits, c->sm_count, d.n_tiles), st);
+            }
             SCB_CUDA(cudaGetLastError());
         }
     }
@@ -390,6 +430,19 @@ scb_status scb_server_create(scb_ctx* ctx, const scb_server_config* cfg_in, scb_
         SCB_CUDA(cudaMallocHost((void**)&s->h_outv, std::max<uint64_t>(B, 1)));
         srv->slots.push_back(std::move(s));
     }
+    if (cfg.spectrum_keys) {
+        uint64_t cap = 1024;
+        while (cap < 2 * cfg.spectrum_keys) cap <<= 1;
+        srv->spectrum = true;
+        srv->spec_mask = cap - 1;
+        srv->spec_dense = ctx->g.bits == 8 ? 256u : 65536u;
+        srv->spec_ovf_cap = ctx->g.bits == 32 ? cfg.spectrum_keys : 1;
+        SCB_TRY(srv->spec_set.ensure(cap * 8));
+        SCB_TRY(srv->spec_hist.ensure((uint64_t)srv->spec_dense * 8));
+        SCB_TRY(srv->spec_ovf.ensure(srv->spec_ovf_cap * 8));
+        SCB_TRY(srv->spec_cnt.ensure(kCntSlots * 8));
+        SCB_TRY(srv->clear_spectrum(srv->slots[0]->stream));
+    }
     scb_server* raw = srv.release();
     raw->worker = std::thread([raw] { raw->run(); });
     *out = raw;
@@ -515,6 +568,64 @@ scb_status scb_server_reset_stats(scb_server* s) {
     s->stat_windows = 0;
     s->stat_batches = 0;
     s->have_first = false;
+    if (s->spectrum) {
+        cudaSetDevice(s->ctx->device);
+        for (auto& sp : s->slots) SCB_CUDA(cudaStreamSynchronize(sp->stream));
+        SCB_TRY(s->clear_spectrum(s->slots[0]->stream));
+    }
+    return SCB_OK;
+}
+
+scb_status scb_server_spectrum(scb_server* s, uint64_t* values, uint64_t* counts, uint64_t capacity,
+                               uint64_t* n_rows, uint64_t* distinct_keys, uint64_t* queried_kmers) {
+    if (!s) return fail_kind(SCB_ERR_INTERNAL_STATE, "null server");
+    if (!s->spectrum) return fail_kind(SCB_ERR_INTERNAL_STATE, "the server was created without spectrum_keys");
+    std::unique_lock<std::mutex> lk(s->mu);
+    // every submitted piece answered: nothing pending, no slot busy
+    s->settled.wait(lk, [&] {
+        if (!s->pending.empty()) return false;
+        for (auto& sp : s->slots) {
+            if (sp->busy) return false;
+        }
+        return true;
+    });
+    cudaSetDevice(s->ctx->device);
+    for (auto& sp : s->slots) SCB_CUDA(cudaStreamSynchronize(sp->stream));
+    cudaStream_t st = s->slots[0]->stream;
+    unsigned long long c[kCntSlots];
+    uint32_t status = 0;
+    std::vector<unsigned long long> dense(s->spec_dense);
+    SCB_CUDA(cudaMemcpyAsync(c, s->spec_cnt.p, kCntSlots * 8, cudaMemcpyDeviceToHost, st));
+    SCB_CUDA(cudaMemcpyAsync(&status, s->ctx->status, 4, cudaMemcpyDeviceToHost, st));
+    SCB_CUDA(cudaMemcpyAsync(dense.data(), s->spec_hist.p, (uint64_t)s->spec_dense * 8, cudaMemcpyDeviceToHost, st));
+    SCB_CUDA(cudaStreamSynchronize(st));
+    if (status) {
+        return fail_kind(SCB_ERR_INTERNAL_STATE, "device status word 0x" + std::to_string(status) +
+                                                     " (2 = the stream has more distinct k-mers than spectrum_keys)");
+    }
+    const uint64_t n_ovf = std::min<uint64_t>(c[kCntOverflow], s->spec_ovf_cap);
+    std::vector<unsigned long long> ovf(n_ovf);
+    if (n_ovf) SCB_CUDA(cudaMemcpy(ovf.data(), s->spec_ovf.p, n_ovf * 8, cudaMemcpyDeviceToHost));
+    std::vector<std::pair<uint64_t, uint64_t>> rows;
+    for (size_t v = 0; v < dense.size(); v++) {
+        if (dense[v]) rows.emplace_back(v, dense[v]);
+    }
+    std::sort(ovf.begin(), ovf.end());
+    for (size_t i = 0; i < ovf.size();) {
+        size_t j = i;
+        while (j < ovf.size() && ovf[j] == ovf[i]) j++;
+        rows.emplace_back(ovf[i], j - i);
+        i = j;
+    }
+    if (distinct_keys) *distinct_keys = c[kCntDistinct];
+    if (queried_kmers) *queried_kmers = c[kCntValid];
+    if (n_rows) *n_rows = rows.size();
+    if (!values || !counts) return SCB_OK;
+    if (capacity < rows.size()) return fail_kind(SCB_ERR_INTERNAL_STATE, "row capacity too small");
+    for (size_t i = 0; i < rows.size(); i++) {
+        values[i] = rows[i].first;
+        counts[i] = rows[i].second;
+    }
     return SCB_OK;
 }
 

@@ -96,3 +96,36 @@ def test_memory_budget_admits_one_small_batch_at_a_time(index_and_requests):
     srv.close()
     with pytest.raises(scb.InvalidConfig, match="budget"):
         scb.SuperCountingBloomServer(idx, memory_budget_bytes=1 << 20, max_batch_bytes=64 << 20)
+
+
+def test_whole_stream_spectrum_equals_batch_spectrum(index_and_requests, oracle_mod):
+    """A server with spectrum_keys adds every answered window's canonical k-mer to one device set;
+    at the end of the stream its spectrum equals the distinct-k-mer spectrum of all the requests'
+    sequences at once (src/fastx.rs:255-308, 392-410), which the oracle checks too."""
+    import scbf_b200 as scb
+
+    idx, requests, expected = index_and_requests
+    srv = scb.SuperCountingBloomServer(idx, max_batch_bytes=2 << 20, max_inflight=4, spectrum_keys=4_000_000)
+    tickets = [srv.submit(d, o) for d, o in requests + requests[:5]]  # repeats add no distinct k-mer
+    for t in tickets:
+        srv.wait(t)
+    got = srv.spectrum()
+    seqs = [bytes(d[int(o[i]):int(o[i + 1])]) for d, o in requests for i in range(len(o) - 1)]
+    data, offsets = scb.pack_sequences(seqs)
+    ref = idx.spectrum_distinct(data, offsets)
+    assert got["rows"] == ref["rows"] and got["distinct_keys"] == ref["distinct_keys"]
+    # every answered valid window is queried once, the five repeated requests' windows again
+    assert got["queried_kmers"] == ref["queried_kmers"] + sum(int(expected[i][1].sum()) for i in range(5))
+    # the oracle's spectrum of the same reads over the same training set
+    from scbf_b200 import workloads
+
+    genome = workloads.random_genome(400_000, seed=31)
+    tr, to = workloads.short_reads(n_reads=30_000, read_len=150, seed=32, sub_rate=0.01, n_rate=0.005, genome=genome)
+    o = oracle_mod.OracleFilter(oracle_mod.make_config(31, 21, 25, 4, 16, 22, 9))
+    o.insert_batch_arrays(tr, to)
+    osp = o.spectrum_distinct_arrays(data, offsets)
+    assert osp["mismatches"] == 0 and got["rows"] == osp["rows"]
+    srv.reset_stats()
+    empty = srv.spectrum()
+    assert empty["rows"] == [] and empty["distinct_keys"] == 0
+    srv.close()
