@@ -56,6 +56,7 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-mixed", action="store_true", help="skip the mixed-length (config 4) comparison")
     p.add_argument("--no-serve", action="store_true", help="skip the serving (config 5) measurement")
+    p.add_argument("--no-spectrum", action="store_true", help="skip the distinct-k-mer spectrum measurement")
     p.add_argument("--no-tune", action="store_true",
                    help="skip the autotuner (untuned defaults: fixed settings for comparing kernel builds)")
     p.add_argument("--profile-case", choices=["plain", "fused", "grouped"], default=None,
@@ -520,6 +521,24 @@ def run_ours(args, dist: Dist):
                 "touched_blocks": touched}
 
     del d_data, d_off
+    spectrum = None
+    if not args.no_spectrum:
+        spectrum = {"config2": run_spectrum(L, h, data, offsets, st, GEOM["counter_slots_exponent"])}
+        # configuration 1: 1 Mbp genome, 30x of 150 bp reads, 2^24 slots (the table fits in L2)
+        from scbf_b200 import workloads as wl
+
+        d1, o1 = wl.config1()
+        cfg1 = api.SuperCountingBloomConfig(k=GEOM["k"], m=GEOM["m"], s=GEOM["s"], n_hashes=GEOM["n_hashes"],
+                                            counter_bits=api.CounterBits(16), counter_slots_exponent=24,
+                                            block_slots_exponent=GEOM["block_slots_exponent"], threads=1, queue=4096)
+        c1 = api._create(cfg1)
+        st1 = _lib.ScbStats()
+        check(L.scb_batch_stats(c1.h, d1.ctypes.data, o1.ctypes.data, len(o1) - 1, C.byref(st1)))
+        k1, s1 = C.c_uint64(0), C.c_uint64(0)
+        check(L.scb_insert_batch(c1.h, d1.ctypes.data, o1.ctypes.data, len(o1) - 1, C.byref(k1), C.byref(s1)))
+        check(L.scb_freeze(c1.h))
+        spectrum["config1"] = run_spectrum(L, c1.h, d1, o1, st1, 24)
+        c1.close()
     serving = None
     if not args.no_serve:
         check(L.scb_set_strategy(h, 0, 0))
@@ -552,11 +571,69 @@ def run_ours(args, dist: Dist):
                                                  "apply_insert_ms", "apply_query_ms")},
             "tuning": tuning, "graphs": graphs,
             "plain": plain, "strategies": strategies, "mixed": mixed, "serve": serving, "e2e": e2e,
+            "spectrum": spectrum,
             "roofline": roofline,
             "cpu_baseline": cpu,
             "clocks": info["clocks"], "gpu_launches": info["launches"],
         }
         print(json.dumps(line), flush=True)
+
+
+def run_spectrum(L, h, data, offsets, st, slot_exp: int, reps: int = 2) -> dict:
+    """estimate_distinct_kmers + spectrum_from_estimates (src/fastx.rs:255-308, 392-410) on the
+    frozen index h over the given reads, through the host entry point scb_spectrum_distinct (reads
+    copied to the device inside the call), with the grouped strategy (the spectrum apply) and the
+    fused tile kernel (one global key-set insert per window).  Algorithmic bytes of the spectrum
+    apply: per super-k-mer its 8-byte record and 2-bit bases, each touched block read once; the
+    keys and the histogram stay on the SM (split buckets excepted)."""
+    from scbf_b200 import _lib
+
+    n = len(offsets) - 1
+    peak, _ = measured_peaks()
+    out = {}
+    ref_rows = None
+    for name in ("grouped", "fused"):
+        sid = STRATEGY_IDS[name]
+        assert L.scb_set_strategy(h, sid, sid) == 0
+        rows, dk, qk = C.c_uint64(0), C.c_uint64(0), C.c_uint64(0)
+        times, dev = [], []
+        for _ in range(reps + 1):
+            assert L.scb_set_timing(h, 1) == 0
+            t0 = time.perf_counter()
+            if L.scb_spectrum_distinct(h, data.ctypes.data, offsets.ctypes.data, n, None, None, 0, C.byref(rows),
+                                       C.byref(dk), C.byref(qk)) != 0:
+                raise RuntimeError(_lib.last_error())
+            times.append(time.perf_counter() - t0)
+            t = _lib.ScbTimings()
+            assert L.scb_get_timings(h, C.byref(t)) == 0
+            dev.append(t.pack_ms + t.query_ms)
+        assert L.scb_set_timing(h, 0) == 0
+        vals, cnts = np.zeros(max(rows.value, 1), np.uint64), np.zeros(max(rows.value, 1), np.uint64)
+        L.scb_spectrum_distinct(h, data.ctypes.data, offsets.ctypes.data, n, vals.ctypes.data, cnts.ctypes.data,
+                                rows.value, C.byref(rows), C.byref(dk), C.byref(qk))
+        got = list(zip(vals[: rows.value].tolist(), cnts[: rows.value].tolist()))
+        if ref_rows is None:
+            ref_rows = got
+        assert got == ref_rows, ("spectrum rows differ between strategies", name)
+        wall = min(times[1:])
+        dms = min(dev[1:])
+        out[name] = {"kmers_per_s": qk.value / wall, "seconds": wall, "device_ms": dms,
+                     "device_kmers_per_s": qk.value / (dms / 1e3) if dms > 0 else None}
+    assert L.scb_set_strategy(h, 0, 0) == 0
+    R = float(st.super_kmers)
+    touched = occupied(R, float(1 << (slot_exp - GEOM["block_slots_exponent"])))
+    block_bytes = (1 << GEOM["block_slots_exponent"]) * (GEOM["counter_bits"] // 8)
+    alg = 8 * R + (st.windows + R * (GEOM["k"] - 1)) / 4.0 + touched * block_bytes + int(offsets[-1]) * 1.5
+    gms = out["grouped"]["device_ms"]
+    out.update({"queried_kmers": qk.value, "distinct_kmers": dk.value, "rows": rows.value,
+                "grouped_over_fused": out["grouped"]["kmers_per_s"] / out["fused"]["kmers_per_s"],
+                "roofline": {"bound": "hbm", "algorithmic_bytes": alg, "device_ms": gms,
+                             "achieved_gbs": alg / (gms / 1e3) / 1e9 if gms else None,
+                             "frac": alg / (gms / 1e3) / 1e9 / peak if gms else None,
+                             "model": "pack (1.5 B per base) + per super-k-mer an 8-byte record and its 2-bit "
+                                      "bases + each touched block read once; keys and histogram stay in shared "
+                                      "memory"}})
+    return out
 
 
 def run_serving(ctx, args, rank: int) -> dict:

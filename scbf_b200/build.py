@@ -16,7 +16,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libscb_b200.so")
 
-SOURCES = ["scb_api.cu", "scb_kernels.cu", "scb_server.cu", "scb_fastx.cu"]
+SOURCES = ["scb_api.cu", "scb_kernels.cu", "scb_server.cu", "scb_fastx.cu", "scb_hostpack.cpp"]
 HEADERS = ["scb_device.cuh", "scb_kernels.cuh", "scb_internal.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3", "--expt-relaxed-constexpr",

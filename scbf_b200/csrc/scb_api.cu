@@ -476,7 +476,7 @@ GroupArgs group_args(const scb_ctx* ctx, const Lane& L, const TileArgs& a, const
 scb_status launch_group_apply(scb_ctx* ctx, Lane& L, int mode, GroupArgs ga, unsigned long long* cnt,
                               uint64_t max_items, cudaStream_t st) {
     ga.cnt = cnt;
-    const bool ins = mode != kModeReport;  // the build apply is timed as the insert apply
+    const bool ins = mode == kModeInsert || mode == kModeBuild;  // the build apply is timed as the insert apply
     SCB_CUDA(cudaMemsetAsync(ga.work_counter, 0, 4, st));
     SCB_TRY(mark(ctx, L, ins ? 7 : 11, st));
     launch_apply(mode, ga, (int)ctx->cfg.block_slots_exponent, 1u << ga.bucket_shift, ctx->sm_count, max_items, st);

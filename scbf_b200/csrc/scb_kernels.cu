@@ -1693,17 +1693,32 @@ __device__ __forceinline__ void apply_body(const GroupArgs& a, uint32_t bs_log2,
                         for (uint32_t vv = w0i; vv < w1i; vv++) wmap[vv] = (uint8_t)tid;
                     }
                     const uint32_t S = spre[nuse];
-                    for (uint32_t f = tid; f < S; f += blockDim.x) {
-                        const unsigned long long pk = __ldcg(kept + qoff + f);
-                        uint32_t e;
-                        if constexpr (NH == 4) {
-                            const uint32_t lo = (uint32_t)pk, hi = (uint32_t)(pk >> 32);
-                            e = min(min(cells[lo & 0xFFFFu], cells[lo >> 16]), min(cells[hi & 0xFFFFu], cells[hi >> 16]));
-                        } else {
-                            e = T::kMax;
-                            for (uint32_t h = 0; h < g.h; h++) e = min(e, (uint32_t)cells[(uint32_t)(pk >> (16 * h)) & 0xFFFFu]);
+                    // kProbeBatch kept probe words in flight per thread (L2 hits: the insert above
+                    // wrote them), then the counter minima from the committed cells
+                    for (uint32_t f0 = tid; f0 < S; f0 += kProbeBatch * blockDim.x) {
+                        unsigned long long pk[kProbeBatch];
+#pragma unroll
+                        for (uint32_t j = 0; j < kProbeBatch; j++) {
+                            const uint32_t f = f0 + j * blockDim.x;
+                            pk[j] = f < S ? __ldcg(kept + qoff + f) : 0ull;
                         }
-                        est[f] = (Est)e;
+#pragma unroll
+                        for (uint32_t j = 0; j < kProbeBatch; j++) {
+                            const uint32_t f = f0 + j * blockDim.x;
+                            if (f >= S) break;
+                            uint32_t e;
+                            if constexpr (NH == 4) {
+                                const uint32_t lo = (uint32_t)pk[j], hi = (uint32_t)(pk[j] >> 32);
+                                e = min(min(cells[lo & 0xFFFFu], cells[lo >> 16]),
+                                        min(cells[hi & 0xFFFFu], cells[hi >> 16]));
+                            } else {
+                                e = T::kMax;
+                                for (uint32_t h = 0; h < g.h; h++) {
+                                    e = min(e, (uint32_t)cells[(uint32_t)(pk[j] >> (16 * h)) & 0xFFFFu]);
+                                }
+                            }
+                            est[f] = (Est)e;
+                        }
                     }
                     __syncthreads();
                     const uint32_t W = wpre[nuse];
