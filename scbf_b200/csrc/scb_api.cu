@@ -1636,29 +1636,35 @@ scb_status scb_spectrum_distinct(scb_ctx* ctx, const uint8_t* seqs, const uint64
     CtxLock lk(ctx);
     SCB_TRY(check_offsets(offsets, n));
     const uint64_t W = windows_of(offsets, n, ctx->cfg.k);
-    uint64_t cap = 1024;
-    while (cap < 2 * W) cap <<= 1;
     DevBuf set, hist, ovf;
     const uint32_t dense = ctx->g.bits == 8 ? 256u : 65536u;
-    SCB_TRY(set.ensure(cap * 8));
     SCB_TRY(hist.ensure((uint64_t)dense * 8));
     const uint64_t ovf_cap = ctx->g.bits == 32 ? std::max<uint64_t>(W, 1) : 1;
     SCB_TRY(ovf.ensure(ovf_cap * 8));
     // the chunks run on the lane's stream, behind these clears
     SCB_TRY(ensure_lane_work(ctx, ctx->lane, 0));
-    SCB_CUDA(cudaMemsetAsync(set.p, 0xFF, cap * 8, ctx->lane.stream));
     SCB_CUDA(cudaMemsetAsync(hist.p, 0, (uint64_t)dense * 8, ctx->lane.stream));
+    // the global key set: twice the keys it can receive, at least 1024 slots, cleared on the
+    // lane's stream
+    uint64_t cap = 0;
+    auto make_set = [&](uint64_t keys) -> scb_status {
+        cap = 1024;
+        while (cap < 2 * keys) cap <<= 1;
+        SCB_TRY(set.ensure(cap * 8));
+        SCB_CUDA(cudaMemsetAsync(set.p, 0xFF, cap * 8, ctx->lane.stream));
+        return SCB_OK;
+    };
     uint64_t distinct = 0, queried = 0, n_ovf = 0;
     // one device batch with the grouped strategy: the spectrum apply deduplicates each exclusive
-    // bucket's keys in shared memory; otherwise the tile kernel inserts every key into the set
+    // bucket's keys in shared memory, so the global set only holds the keys of split buckets;
+    // otherwise the tile kernel inserts every key into a set sized for all the windows
     std::vector<Chunk> plan;
     SCB_TRY(plan_chunks(offsets, n, ctx->cfg.k, ctx->tuning.host_batch_bytes, plan));
     const uint64_t total = n ? offsets[n] - offsets[0] : 0;
     const bool grouped = plan.size() == 1 && grouped_supported(ctx) &&
                          resolve(ctx, ctx->query_strategy, total, false) == SCB_STRATEGY_GROUPED;
+    if (!grouped) SCB_TRY(make_set(W));
     SCB_TRY(for_each_chunk(ctx, seqs, offsets, n, [&](Lane& L, TileArgs& a, const Chunk&) -> scb_status {
-        a.set_keys = set.as<unsigned long long>();
-        a.set_mask = cap - 1;
         a.hist = hist.as<unsigned long long>();
         a.hist_dense = dense;
         a.ovf = ovf.as<unsigned long long>() + n_ovf;
@@ -1670,6 +1676,16 @@ scb_status scb_spectrum_distinct(scb_ctx* ctx, const uint8_t* seqs, const uint64
             L.want_spectrum = false;
             SCB_TRY(rs);
             if (L.gs.produced) {
+                // windows of the split buckets' items bound the global set
+                unsigned long long* cnt = L.rec_count.as<unsigned long long>() + 3;
+                unsigned long long shared_windows = 0;
+                SCB_CUDA(cudaMemsetAsync(cnt, 0, 8, L.stream));
+                launch_shared_item_windows(L.gs.ga.items, L.gs.ga.n_items, L.gs.ga.recs, cnt, L.stream);
+                SCB_CUDA(cudaMemcpyAsync(&shared_windows, cnt, 8, cudaMemcpyDeviceToHost, L.stream));
+                SCB_CUDA(cudaStreamSynchronize(L.stream));
+                SCB_TRY(make_set(shared_windows));
+                a.set_keys = set.as<unsigned long long>();
+                a.set_mask = cap - 1;
                 GroupArgs ga = L.gs.ga;
                 ga.set_keys = a.set_keys;
                 ga.set_mask = a.set_mask;
@@ -1683,6 +1699,8 @@ scb_status scb_spectrum_distinct(scb_ctx* ctx, const uint8_t* seqs, const uint64
             SCB_TRY(mark(ctx, L, 10, L.stream));
             if (ctx->timing) L.spans |= kSpanQuery;
         } else {
+            a.set_keys = set.as<unsigned long long>();
+            a.set_mask = cap - 1;
             SCB_TRY(query_device_batch(ctx, L, kModeDistinct, a, L.stream));
         }
         unsigned long long c[kCntSlots];

@@ -382,9 +382,9 @@ __device__ __forceinline__ void nt_direct_tab(const TileSmem& sm, uint64_t v, ui
 }
 
 // Block id of the super-k-mer whose minimizer m-mer starts at relative base b.
-__device__ __forceinline__ uint32_t minimizer_block(const uint32_t* codes_s, uint32_t b, const DevGeom& g) {
-    const uint64_t mm = codes64(codes_s, b) & len_mask(g.m);
-    return (uint32_t)(xorshift64(canonical(mm, g.m)) & g.block_mask);
+__device__ __forceinline__ uint32_t minimizer_block(const uint32_t* codes_s, uint32_t b, uint32_t m, uint64_t block_mask) {
+    const uint64_t mm = codes64(codes_s, b) & len_mask(m);
+    return (uint32_t)(xorshift64(canonical(mm, m)) & block_mask);
 }
 
 __device__ __forceinline__ uint32_t code_at(const uint32_t* words, uint32_t b) {
@@ -470,15 +470,20 @@ __device__ __forceinline__ uint32_t window_estimate(const TileArgs& a, const Dev
     return r;
 }
 
-template <int MODE, int BITS>
+// KMC: 0 for any k and m, or (k << 8) | m compiled in (the cut of the default geometry, k = 31,
+// m = 21, w = 11: the window-minimum strips unroll and the k- and m-masks are constants).
+template <int MODE, int BITS, int KMC = 0>
 __global__ void __launch_bounds__(kTileThreads, 8) k_tiles(TileArgs a) {
     __shared__ TileSmem sm;
     const DevGeom g = a.g;
+    const uint32_t kv = KMC ? (uint32_t)(KMC >> 8) : g.k;
+    const uint32_t mv = KMC ? (uint32_t)(KMC & 255) : g.m;
+    const uint32_t wv = kv - mv + 1;
     const uint32_t tid = threadIdx.x;
     uint32_t* table32 = reinterpret_cast<uint32_t*>(a.table);
     unsigned long long c_win = 0, c_smer = 0, c_valid = 0, c_pos = 0, c_sum = 0, c_sk = 0, c_sec = 0, c_dist = 0;
     const uint64_t s_mask = len_mask(g.s);
-    const uint32_t ks = g.k - g.s;
+    const uint32_t ks = kv - g.s;
     // modes that read a block id for every valid window (the cut computes it at ends only)
     constexpr bool kBlockPerWindow = MODE == kModeInsert || MODE == kModeReport || MODE == kModeAbund ||
                                      MODE == kModeDistinct || MODE == kModeMaterialize;
@@ -496,7 +501,7 @@ __global__ void __launch_bounds__(kTileThreads, 8) k_tiles(TileArgs a) {
     }
     constexpr uint32_t kWin = MODE == kModeCut ? (uint32_t)kCutWindows : (uint32_t)kTileWindows;  // tile windows
     if constexpr (MODE == kModeCut) n_tiles = (uint32_t)((n_bytes + kWin - 1) / kWin);
-    fill_nt_tables(sm, g.m);
+    fill_nt_tables(sm, mv);
 
     while (true) {
         if (tid == 0) sm.tile = atomicAdd(a.tile_counter, 1u);
@@ -509,7 +514,7 @@ __global__ void __launch_bounds__(kTileThreads, 8) k_tiles(TileArgs a) {
                                   : 0u;
         const uint64_t e0 = t0 - back;
         const uint32_t n_eval = MODE == kModeCut ? (uint32_t)kTileWindows : back + kTileWindows + kFwd;
-        const uint32_t n_keys = n_eval + g.w - 1;
+        const uint32_t n_keys = n_eval + wv - 1;
 
         // stage codes and bitmaps of the tile
         const uint64_t cb = e0 & ~15ull;
@@ -544,9 +549,9 @@ __global__ void __launch_bounds__(kTileThreads, 8) k_tiles(TileArgs a) {
                 const uint64_t b0 = e0 + q0 - cb;
                 uint32_t fw, rc;
                 uint64_t outs = codes64(sm.codes, b0);  // bases leaving: b0, b0+1, ...
-                nt_direct_tab(sm, outs & len_mask(g.m), g.m, fw, rc);
+                nt_direct_tab(sm, outs & len_mask(mv), mv, fw, rc);
                 sm.pk[q0] = ((fw + rc) & 0xFFFF0000u) | q0;
-                uint64_t ins = codes64(sm.codes, b0 + g.m);  // bases entering: b0+m, b0+m+1, ...
+                uint64_t ins = codes64(sm.codes, b0 + mv);  // bases entering: b0+m, b0+m+1, ...
                 for (uint32_t q = q0 + 1; q < q1; q++) {
                     const uint32_t idx = ((uint32_t)outs & 3u) | (((uint32_t)ins & 3u) << 2);
                     outs >>= 2;
@@ -562,24 +567,24 @@ __global__ void __launch_bounds__(kTileThreads, 8) k_tiles(TileArgs a) {
         // (b) minimizer of each evaluated window: leftmost minimum = min(pk), rightmost minimum =
         // min(pk ^ 0xFFFF) (the position bits inverted); strand from the count of T/G bases.
         // Windows 0..1023 go in strips of four per thread; the rest (and w < 4) one at a time.
-        const uint32_t strip_end = g.w >= 4 ? (uint32_t)kTileWindows : 0u;
+        const uint32_t strip_end = wv >= 4 ? (uint32_t)kTileWindows : 0u;
         if (strip_end) {
             const uint32_t i0 = 4 * tid;
             const uint64_t pos0 = e0 + i0;
             const uint64_t vb = bits64(sm.valid, pos0 - bb), sb = bits64(sm.start, pos0 - bb);
             uint32_t lm[4], rm[4];
-            strip_minima(sm.pk, i0, g.w, lm, rm);
-            uint32_t tg = __popcll(codes64(sm.codes, pos0 - cb) & len_mask(g.k) & 0xAAAAAAAAAAAAAAAAull);
+            strip_minima(sm.pk, i0, wv, lm, rm);
+            uint32_t tg = __popcll(codes64(sm.codes, pos0 - cb) & len_mask(kv) & 0xAAAAAAAAAAAAAAAAull);
 #pragma unroll
             for (uint32_t j = 0; j < 4; j++) {
                 if (j > 0) {  // roll the T/G count by one base
                     const uint64_t out_b = pos0 + j - 1 - cb;
-                    tg += (code_at(sm.codes, out_b + g.k) >> 1) - (code_at(sm.codes, out_b) >> 1);
+                    tg += (code_at(sm.codes, out_b + kv) >> 1) - (code_at(sm.codes, out_b) >> 1);
                 }
                 uint16_t po = kNoWindow;
-                if (window_ok(vb >> j, sb >> j, g.k)) {
-                    po = (uint16_t)((2 * tg > g.k) ? (lm[j] & 0xFFFFu) : ((rm[j] & 0xFFFFu) ^ 0xFFFFu));
-                    if constexpr (kBlockPerWindow) sm.block[i0 + j] = minimizer_block(sm.codes, e0 + po - cb, g);
+                if (window_ok(vb >> j, sb >> j, kv)) {
+                    po = (uint16_t)((2 * tg > kv) ? (lm[j] & 0xFFFFu) : ((rm[j] & 0xFFFFu) ^ 0xFFFFu));
+                    if constexpr (kBlockPerWindow) sm.block[i0 + j] = minimizer_block(sm.codes, e0 + po - cb, mv, g.block_mask);
                 }
                 sm.poff[i0 + j] = po;
             }
@@ -587,17 +592,17 @@ __global__ void __launch_bounds__(kTileThreads, 8) k_tiles(TileArgs a) {
         for (uint32_t i = strip_end + tid; i < n_eval; i += blockDim.x) {
             const uint64_t pos = e0 + i;
             uint16_t po = kNoWindow;
-            if (window_ok(bits64(sm.valid, pos - bb), bits64(sm.start, pos - bb), g.k)) {
+            if (window_ok(bits64(sm.valid, pos - bb), bits64(sm.start, pos - bb), kv)) {
                 uint32_t lmin = 0xFFFFFFFFu, rmin = 0xFFFFFFFFu;
-                for (uint32_t o = 0; o < g.w; o++) {
+                for (uint32_t o = 0; o < wv; o++) {
                     const uint32_t p = sm.pk[i + o];
                     lmin = min(lmin, p);
                     rmin = min(rmin, p ^ 0xFFFFu);
                 }
-                const uint64_t kv = codes64(sm.codes, pos - cb) & len_mask(g.k);
-                const uint32_t tg = __popcll(kv & 0xAAAAAAAAAAAAAAAAull);
-                po = (uint16_t)((2 * tg > g.k) ? (lmin & 0xFFFFu) : ((rmin & 0xFFFFu) ^ 0xFFFFu));
-                if constexpr (kBlockPerWindow) sm.block[i] = minimizer_block(sm.codes, e0 + po - cb, g);
+                const uint64_t kval = codes64(sm.codes, pos - cb) & len_mask(kv);
+                const uint32_t tg = __popcll(kval & 0xAAAAAAAAAAAAAAAAull);
+                po = (uint16_t)((2 * tg > kv) ? (lmin & 0xFFFFu) : ((rmin & 0xFFFFu) ^ 0xFFFFu));
+                if constexpr (kBlockPerWindow) sm.block[i] = minimizer_block(sm.codes, e0 + po - cb, mv, g.block_mask);
             }
             sm.poff[i] = po;
         }
@@ -643,7 +648,7 @@ __global__ void __launch_bounds__(kTileThreads, 8) k_tiles(TileArgs a) {
                     a.out_valid[o] = 1;
                 } else {
                     c_valid++;
-                    const uint64_t key = canonical(codes64(sm.codes, pos - cb) & len_mask(g.k), g.k);
+                    const uint64_t key = canonical(codes64(sm.codes, pos - cb) & len_mask(kv), kv);
                     if (set_insert(a.set_keys, a.set_mask, key, a.status)) {
                         c_dist++;
                         if (r < a.hist_dense) {
@@ -764,7 +769,7 @@ __global__ void __launch_bounds__(kTileThreads, 8) k_tiles(TileArgs a) {
                 const uint32_t nwin = i - st + 1;
                 c_sk++;
                 c_smer += nwin + ks;
-                const uint32_t block = minimizer_block(sm.codes, e0 + po - cb, g);
+                const uint32_t block = minimizer_block(sm.codes, e0 + po - cb, mv, g.block_mask);
                 const unsigned long long val =
                     (unsigned long long)(e0 + st) | ((unsigned long long)nwin << kRecWindowsShift);
                 // the super-k-mer's bases (64 from its first one) travel with the record, so the
@@ -815,10 +820,19 @@ __global__ void __launch_bounds__(kTileThreads, 8) k_tiles(TileArgs a) {
 
 template <int MODE>
 static void launch_tiles_bits(const TileArgs& a, int grid, cudaStream_t st) {
-    switch (a.g.bits) {
-        case 8: k_tiles<MODE, 8><<<grid, kTileThreads, 0, st>>>(a); break;
-        case 16: k_tiles<MODE, 16><<<grid, kTileThreads, 0, st>>>(a); break;
-        default: k_tiles<MODE, 32><<<grid, kTileThreads, 0, st>>>(a); break;
+    constexpr int kDefaultKM = (31 << 8) | 21;
+    if (MODE == kModeCut && (((int)a.g.k << 8) | (int)a.g.m) == kDefaultKM) {
+        switch (a.g.bits) {
+            case 8: k_tiles<MODE, 8, kDefaultKM><<<grid, kTileThreads, 0, st>>>(a); break;
+            case 16: k_tiles<MODE, 16, kDefaultKM><<<grid, kTileThreads, 0, st>>>(a); break;
+            default: k_tiles<MODE, 32, kDefaultKM><<<grid, kTileThreads, 0, st>>>(a); break;
+        }
+    } else {
+        switch (a.g.bits) {
+            case 8: k_tiles<MODE, 8><<<grid, kTileThreads, 0, st>>>(a); break;
+            case 16: k_tiles<MODE, 16><<<grid, kTileThreads, 0, st>>>(a); break;
+            default: k_tiles<MODE, 32><<<grid, kTileThreads, 0, st>>>(a); break;
+        }
     }
     note_launch();
 }
@@ -1083,6 +1097,29 @@ __global__ void k_item_write(const unsigned long long* __restrict__ counts, uint
     }
 }
 
+// Windows of the work items whose keys go to the global set of the spectrum apply: those that are
+// not their bucket's only one, and those with more than kSpecSet / 2 windows (too many for the
+// shared-memory set).  One thread per item, summed into *out.
+__global__ void k_shared_item_windows(const uint4* __restrict__ items, const unsigned long long* __restrict__ n_items,
+                                      const unsigned long long* __restrict__ recs, unsigned long long* out) {
+    const uint64_t n = *n_items;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    unsigned long long sum = 0;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const uint4 it = items[i];
+        unsigned long long wins = 0;
+        for (uint32_t r = 0; r < it.z; r++) wins += (recs[it.y + r] >> kRecWindowsShift) & 63u;
+        if (!it.w || 2 * wins > kSpecSet) sum += wins;
+    }
+    warp_add_u64(out, sum);
+}
+
+void launch_shared_item_windows(const uint4* items, const unsigned long long* n_items, const unsigned long long* recs,
+                                unsigned long long* out, cudaStream_t st) {
+    k_shared_item_windows<<<592, 256, 0, st>>>(items, n_items, recs, out);
+    note_launch();
+}
+
 // Largest r in [0, n) with pre[r] <= v (pre[0] = 0, pre non-decreasing).
 __device__ __forceinline__ uint32_t find_rec(const uint32_t* pre, uint32_t n, uint32_t v) {
     uint32_t lo = 0, hi = n - 1;
@@ -1235,10 +1272,113 @@ __device__ __forceinline__ bool smem_set_insert(unsigned long long* keys, uint32
     return false;
 }
 
+// Commits a work item's u32 deltas (cells, bucket_blocks blocks of 2^bs_log2 counters) to the
+// table: min(old + delta, MAX) per counter (counter.rs saturation), 16 bytes per thread when the
+// item is its bucket's only one, 32-bit words when blocks are word-aligned, saturating CAS per
+// counter otherwise (items of a split bucket commit concurrently).  keep_finals (an exclusive item
+// only) leaves each touched counter's committed value in its cell.
+template <int BITS>
+__device__ __forceinline__ void commit_item(uint32_t* cells, const uint8_t* touched, const GroupArgs& a,
+                                            uint64_t bucket, uint32_t bs_log2, uint32_t bucket_blocks,
+                                            bool exclusive, bool keep_finals) {
+    using T = CounterTraits<BITS>;
+    using Cnt = typename CounterType<BITS>::type;
+    constexpr uint32_t kVecLog2 = BITS == 8 ? 4u : (BITS == 16 ? 3u : 2u);
+    constexpr uint32_t lanes = T::kLanes;
+    const DevGeom& g = a.g;
+    const uint32_t tid = threadIdx.x;
+    const uint32_t bs = 1u << bs_log2;
+    const uint32_t bucket_slots = bs * bucket_blocks;
+    uint32_t* table32 = reinterpret_cast<uint32_t*>(a.table);
+    const bool word_ok = exclusive && (bs % lanes) == 0;
+    if (exclusive && bs_log2 >= kVecLog2) {
+        // 16 bytes of the table per thread: kVec counters, their u32 deltas in shared memory
+        constexpr uint32_t kVec = 1u << kVecLog2;
+        const uint32_t vlog = bs_log2 - kVecLog2;
+        const uint32_t n_vec = bucket_blocks << vlog;
+        const uint4* d4 = reinterpret_cast<const uint4*>(cells);
+        for (uint32_t x = tid; x < n_vec; x += blockDim.x) {
+            const uint32_t lb = x >> vlog;
+            if (!touched[lb]) continue;
+            const uint64_t base = block_base(g, (bucket << a.bucket_shift) | lb);
+            uint4* wp = reinterpret_cast<uint4*>(reinterpret_cast<Cnt*>(a.table) + base) + (x & ((1u << vlog) - 1u));
+            const uint4 o4 = __ldcg(wp);
+            uint32_t d[kVec];
+#pragma unroll
+            for (uint32_t q = 0; q < kVec / 4; q++) {
+                const uint4 v = d4[x * (kVec / 4) + q];
+                d[4 * q] = v.x;
+                d[4 * q + 1] = v.y;
+                d[4 * q + 2] = v.z;
+                d[4 * q + 3] = v.w;
+            }
+            const uint32_t ow[4] = {o4.x, o4.y, o4.z, o4.w};
+            uint32_t nw[4];
+#pragma unroll
+            for (uint32_t w = 0; w < 4; w++) {
+                uint32_t acc = 0;
+#pragma unroll
+                for (uint32_t l = 0; l < lanes; l++) {
+                    const uint64_t cur = (ow[w] >> (l * BITS)) & T::kMax;
+                    const uint64_t sum = cur + d[w * lanes + l];
+                    acc |= (uint32_t)(sum < T::kMax ? sum : T::kMax) << (l * BITS);
+                }
+                nw[w] = acc;
+            }
+            __stcg(wp, make_uint4(nw[0], nw[1], nw[2], nw[3]));
+            if (keep_finals) {
+                uint4* c4w = reinterpret_cast<uint4*>(cells);
+#pragma unroll
+                for (uint32_t q = 0; q < kVec / 4; q++) {
+                    uint32_t fv[4];
+#pragma unroll
+                    for (uint32_t j = 0; j < 4; j++) {
+                        const uint32_t c = 4 * q + j;  // counter c of the vector: word c / lanes
+                        fv[j] = (nw[c / lanes] >> ((c % lanes) * BITS)) & T::kMax;
+                    }
+                    c4w[x * (kVec / 4) + q] = make_uint4(fv[0], fv[1], fv[2], fv[3]);
+                }
+            }
+        }
+    } else if (word_ok) {
+        const uint32_t block_words = bs / lanes;
+        for (uint32_t x = tid; x < bucket_blocks * block_words; x += blockDim.x) {
+            const uint32_t lb = x / block_words, wi = x % block_words;
+            if (!touched[lb]) continue;
+            const uint64_t base = block_base(g, (bucket << a.bucket_shift) | lb);
+            uint32_t* wp = table32 + base / lanes + wi;
+            const uint32_t old = __ldcg(wp);
+            uint32_t nw = 0;
+            const uint32_t cb = (lb << bs_log2) + wi * lanes;
+#pragma unroll
+            for (uint32_t l = 0; l < lanes; l++) {
+                const uint64_t cur = (old >> (l * BITS)) & T::kMax;
+                const uint64_t sum = cur + cells[cb + l];
+                const uint32_t nv = (uint32_t)(sum < T::kMax ? sum : T::kMax);
+                nw |= nv << (l * BITS);
+                if (keep_finals) cells[cb + l] = nv;
+            }
+            __stcg(wp, nw);
+        }
+    } else {
+        for (uint32_t x = tid; x < bucket_slots; x += blockDim.x) {
+            const uint32_t lb = x >> bs_log2;
+            const uint32_t d = cells[x];
+            if (!touched[lb] || d == 0) continue;
+            const uint64_t base = block_base(g, (bucket << a.bucket_shift) | lb);
+            sat_add<BITS>(table32, base + (x & (bs - 1)), d, a.status);
+        }
+    }
+}
+
 // NH = 4: four hashes per s-mer (the default geometry), unrolled; NH = 0: any n_hashes.  Kept
 // probe slots are 16-bit lanes (n_hashes <= 4), each the counter's index within the bucket's
 // shared-memory cells, so the query needs neither the s-mer nor its record.
-template <int MODE, int BITS, int NH, bool LEAN>
+// KSC: 0 for any k and s, or (k << 8) | s of the default geometry (k = 31, s = 25) compiled in, so
+// that the s-mer and window loops and masks are constants (measured 4-5 % faster).
+constexpr int kDefaultKS = (31 << 8) | 25;
+
+template <int MODE, int BITS, int NH, bool LEAN, int KSC = 0>
 __device__ __forceinline__ void apply_body(const GroupArgs& a, uint32_t bs_log2, uint32_t bucket_blocks) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     using T = CounterTraits<BITS>;
@@ -1278,9 +1418,10 @@ __device__ __forceinline__ void apply_body(const GroupArgs& a, uint32_t bs_log2,
     __shared__ uint32_t warp_tot[2 * (kApplyMaxThreads / 32)];
 
     const uint32_t tid = threadIdx.x;
-    const uint32_t ks = g.k - g.s;
-    const uint64_t s_mask = len_mask(g.s);
-    uint32_t* table32 = reinterpret_cast<uint32_t*>(a.table);
+    const uint32_t kv = KSC ? (uint32_t)(KSC >> 8) : g.k;
+    const uint32_t sv = KSC ? (uint32_t)(KSC & 255) : g.s;
+    const uint32_t ks = kv - sv;
+    const uint64_t s_mask = len_mask(sv);
     const uint64_t n_items = *a.n_items;
     if (a.rec_count && *a.rec_count > a.rec_cap) return;  // records outgrew their slots: host redoes it
     unsigned long long c_valid = 0, c_pos = 0, c_sum = 0, c_dist = 0;
@@ -1482,10 +1623,10 @@ __device__ __forceinline__ void apply_body(const GroupArgs& a, uint32_t bs_log2,
                 // read past the record's words land above 2s and are masked off)
                 uint64_t smer;
                 if constexpr (LEAN) {  // no staged bases: the codes from global memory
-                    smer = canonical(codes64(a.codes, start + (f - spre[r])) & s_mask, g.s);
+                    smer = canonical(codes64(a.codes, start + (f - spre[r])) & s_mask, sv);
                 } else {
                     const uint64_t fw = codes64(bases + r * kRecBaseWords, rel) & s_mask;
-                    const uint64_t rc = codes64(rbases + r * kRecBaseWords, 16u * kRecBaseWords - rel - g.s) & s_mask;
+                    const uint64_t rc = codes64(rbases + r * kRecBaseWords, 16u * kRecBaseWords - rel - sv) & s_mask;
                     smer = fw < rc ? fw : rc;
                 }
                 uint64_t hash = xorshift64(smer);
@@ -1556,7 +1697,7 @@ __device__ __forceinline__ void apply_body(const GroupArgs& a, uint32_t bs_log2,
                 // fastx.rs:255-308, 392-410: each window's canonical k-mer (from the staged bases
                 // and their mirror) counts its estimate once, the first time the key is seen
                 const uint32_t W = wpre[nrec_used];
-                const uint64_t kmask = len_mask(g.k);
+                const uint64_t kmask = len_mask(kv);
                 for (uint32_t v = tid; v < W; v += blockDim.x) {
                     const uint32_t r = wmap[v];
                     const uint32_t off = v - wpre[r];
@@ -1564,7 +1705,7 @@ __device__ __forceinline__ void apply_body(const GroupArgs& a, uint32_t bs_log2,
                     uint32_t m = e[0];
                     for (uint32_t t = 1; t <= ks; t++) m = min(m, (uint32_t)e[t]);
                     const uint64_t fw = codes64(bases + r * kRecBaseWords, off) & kmask;
-                    const uint64_t rc = codes64(rbases + r * kRecBaseWords, 16u * kRecBaseWords - off - g.k) & kmask;
+                    const uint64_t rc = codes64(rbases + r * kRecBaseWords, 16u * kRecBaseWords - off - kv) & kmask;
                     const uint64_t key = fw < rc ? fw : rc;
                     c_valid++;
                     const bool fresh = set_cap ? smem_set_insert(skeys, set_cap - 1, key)
@@ -1592,88 +1733,7 @@ __device__ __forceinline__ void apply_body(const GroupArgs& a, uint32_t bs_log2,
         }
 
         if constexpr (kDeltas) {
-            // commit the deltas: min(old + delta, MAX) per counter (counter.rs saturation); a
-            // build item that answers its own query keeps the committed values in its cells
-            constexpr uint32_t lanes = T::kLanes;
-            const bool word_ok = exclusive && (bs % lanes) == 0;
-            if (exclusive && bs_log2 >= kVecLog2) {
-                // 16 bytes of the table per thread: kVec counters, their u32 deltas in shared memory
-                constexpr uint32_t kVec = 1u << kVecLog2;
-                const uint32_t vlog = bs_log2 - kVecLog2;
-                const uint32_t n_vec = bucket_blocks << vlog;
-                const uint4* d4 = reinterpret_cast<const uint4*>(cells);
-                for (uint32_t x = tid; x < n_vec; x += blockDim.x) {
-                    const uint32_t lb = x >> vlog;
-                    if (!touched[lb]) continue;
-                    const uint64_t base = block_base(g, (bucket << a.bucket_shift) | lb);
-                    uint4* wp = reinterpret_cast<uint4*>(reinterpret_cast<Cnt*>(a.table) + base) + (x & ((1u << vlog) - 1u));
-                    const uint4 o4 = __ldcg(wp);
-                    uint32_t d[kVec];
-#pragma unroll
-                    for (uint32_t q = 0; q < kVec / 4; q++) {
-                        const uint4 v = d4[x * (kVec / 4) + q];
-                        d[4 * q] = v.x;
-                        d[4 * q + 1] = v.y;
-                        d[4 * q + 2] = v.z;
-                        d[4 * q + 3] = v.w;
-                    }
-                    const uint32_t ow[4] = {o4.x, o4.y, o4.z, o4.w};
-                    uint32_t nw[4];
-#pragma unroll
-                    for (uint32_t w = 0; w < 4; w++) {
-                        uint32_t acc = 0;
-#pragma unroll
-                        for (uint32_t l = 0; l < lanes; l++) {
-                            const uint64_t cur = (ow[w] >> (l * BITS)) & T::kMax;
-                            const uint64_t sum = cur + d[w * lanes + l];
-                            acc |= (uint32_t)(sum < T::kMax ? sum : T::kMax) << (l * BITS);
-                        }
-                        nw[w] = acc;
-                    }
-                    __stcg(wp, make_uint4(nw[0], nw[1], nw[2], nw[3]));
-                    if (kBuild && fused) {
-                        uint4* c4w = reinterpret_cast<uint4*>(cells);
-#pragma unroll
-                        for (uint32_t q = 0; q < kVec / 4; q++) {
-                            uint32_t fv[4];
-#pragma unroll
-                            for (uint32_t j = 0; j < 4; j++) {
-                                const uint32_t c = 4 * q + j;  // counter c of the vector: word c / lanes
-                                fv[j] = (nw[c / lanes] >> ((c % lanes) * BITS)) & T::kMax;
-                            }
-                            c4w[x * (kVec / 4) + q] = make_uint4(fv[0], fv[1], fv[2], fv[3]);
-                        }
-                    }
-                }
-            } else if (word_ok) {
-                const uint32_t block_words = bs / lanes;
-                for (uint32_t x = tid; x < bucket_blocks * block_words; x += blockDim.x) {
-                    const uint32_t lb = x / block_words, wi = x % block_words;
-                    if (!touched[lb]) continue;
-                    const uint64_t base = block_base(g, (bucket << a.bucket_shift) | lb);
-                    uint32_t* wp = table32 + base / lanes + wi;
-                    const uint32_t old = __ldcg(wp);
-                    uint32_t nw = 0;
-                    const uint32_t cb = (lb << bs_log2) + wi * lanes;
-#pragma unroll
-                    for (uint32_t l = 0; l < lanes; l++) {
-                        const uint64_t cur = (old >> (l * BITS)) & T::kMax;
-                        const uint64_t sum = cur + cells[cb + l];
-                        const uint32_t nv = (uint32_t)(sum < T::kMax ? sum : T::kMax);
-                        nw |= nv << (l * BITS);
-                        if (kBuild && fused) cells[cb + l] = nv;
-                    }
-                    __stcg(wp, nw);
-                }
-            } else {
-                for (uint32_t x = tid; x < bucket_slots; x += blockDim.x) {
-                    const uint32_t lb = x >> bs_log2;
-                    const uint32_t d = cells[x];
-                    if (!touched[lb] || d == 0) continue;
-                    const uint64_t base = block_base(g, (bucket << a.bucket_shift) | lb);
-                    sat_add<BITS>(table32, base + (x & (bs - 1)), d, a.status);
-                }
-            }
+            commit_item<BITS>(cells, touched, a, bucket, bs_log2, bucket_blocks, exclusive, kBuild && fused);
         }
         if constexpr (kBuild) {
             if (fused) {
@@ -1753,25 +1813,25 @@ __device__ __forceinline__ void apply_body(const GroupArgs& a, uint32_t bs_log2,
     }
 }
 
-template <int MODE, int BITS, int NH>
+template <int MODE, int BITS, int NH, int KSC>
 __global__ void __launch_bounds__(kApplyMaxThreads) k_apply_insert(GroupArgs a, uint32_t bs_log2,
                                                                     uint32_t bucket_blocks) {
-    apply_body<MODE, BITS, NH, false>(a, bs_log2, bucket_blocks);
+    apply_body<MODE, BITS, NH, false, KSC>(a, bs_log2, bucket_blocks);
 }
 
 // The query is held to 2048 threads per SM at every CTA width (at most 32 registers), which
 // measured faster than the compiler's own choice; the insert measured faster without it.
-template <int MODE, int BITS, int NH, bool LEAN>
+template <int MODE, int BITS, int NH, bool LEAN, int KSC>
 __global__ void __launch_bounds__(kApplyMaxThreads, 2048 / kApplyMaxThreads) k_apply_query(GroupArgs a,
                                                                                            uint32_t bs_log2,
                                                                                            uint32_t bucket_blocks) {
-    apply_body<MODE, BITS, NH, LEAN>(a, bs_log2, bucket_blocks);
+    apply_body<MODE, BITS, NH, LEAN, KSC>(a, bs_log2, bucket_blocks);
 }
 
-template <int MODE, int BITS, int NH>
+template <int MODE, int BITS, int NH, int KSC>
 __global__ void __launch_bounds__(kApplyMaxThreads) k_apply_spectrum(GroupArgs a, uint32_t bs_log2,
                                                                       uint32_t bucket_blocks) {
-    apply_body<MODE, BITS, NH, false>(a, bs_log2, bucket_blocks);
+    apply_body<MODE, BITS, NH, false, KSC>(a, bs_log2, bucket_blocks);
 }
 
 static size_t apply_smem(int mode, int bits, uint32_t bucket_slots, uint32_t bucket_blocks, bool lean) {
@@ -1784,15 +1844,20 @@ static void launch_apply_t(const GroupArgs& a, int bs_log2, uint32_t bucket_bloc
     const bool lean = MODE == kModeReport && a.probes != nullptr;
     const size_t smem = apply_smem(MODE, BITS, (1u << bs_log2) * bucket_blocks, bucket_blocks, lean);
     void (*fn)(GroupArgs, uint32_t, uint32_t);
+    const bool dflt = a.g.h == 4 && (((int)a.g.k << 8) | (int)a.g.s) == kDefaultKS;
     if constexpr (MODE == kModeInsert || MODE == kModeBuild) {
-        fn = a.g.h == 4 ? k_apply_insert<MODE, BITS, 4> : k_apply_insert<MODE, BITS, 0>;
+        fn = dflt ? k_apply_insert<MODE, BITS, 4, kDefaultKS>
+                  : (a.g.h == 4 ? k_apply_insert<MODE, BITS, 4, 0> : k_apply_insert<MODE, BITS, 0, 0>);
     } else if constexpr (MODE == kModeSpectrum) {
-        fn = a.g.h == 4 ? k_apply_spectrum<MODE, BITS, 4> : k_apply_spectrum<MODE, BITS, 0>;
+        fn = dflt ? k_apply_spectrum<MODE, BITS, 4, kDefaultKS>
+                  : (a.g.h == 4 ? k_apply_spectrum<MODE, BITS, 4, 0> : k_apply_spectrum<MODE, BITS, 0, 0>);
     } else {
         if (lean) {
-            fn = a.g.h == 4 ? k_apply_query<MODE, BITS, 4, true> : k_apply_query<MODE, BITS, 0, true>;
+            fn = dflt ? k_apply_query<MODE, BITS, 4, true, kDefaultKS>
+                      : (a.g.h == 4 ? k_apply_query<MODE, BITS, 4, true, 0> : k_apply_query<MODE, BITS, 0, true, 0>);
         } else {
-            fn = a.g.h == 4 ? k_apply_query<MODE, BITS, 4, false> : k_apply_query<MODE, BITS, 0, false>;
+            fn = dflt ? k_apply_query<MODE, BITS, 4, false, kDefaultKS>
+                      : (a.g.h == 4 ? k_apply_query<MODE, BITS, 4, false, 0> : k_apply_query<MODE, BITS, 0, false, 0>);
         }
     }
     cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -1808,6 +1873,8 @@ static void launch_apply_t(const GroupArgs& a, int bs_log2, uint32_t bucket_bloc
     fn<<<(unsigned)grid, threads, smem, st>>>(a, (uint32_t)bs_log2, bucket_blocks);
     note_launch();
 }
+
+
 
 void launch_apply(int mode, const GroupArgs& a, int bs_log2, uint32_t bucket_blocks, int sm_count, uint64_t max_items,
                   cudaStream_t st) {

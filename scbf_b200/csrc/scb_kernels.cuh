@@ -217,6 +217,8 @@ void launch_item_write(const unsigned long long* counts, uint64_t bucket_cap, co
                        cudaStream_t st);
 void launch_apply(int mode, const GroupArgs& a, int block_slots, uint32_t bucket_blocks, int sm_count,
                   uint64_t max_items, cudaStream_t st);
+void launch_shared_item_windows(const uint4* items, const unsigned long long* n_items, const unsigned long long* recs,
+                                unsigned long long* out, cudaStream_t st);
 
 uint64_t kernel_launch_count();
 void note_launch();
