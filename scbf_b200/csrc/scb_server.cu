@@ -13,7 +13,9 @@
 // Batches of different slots overlap on the GPU; requests that arrive while
 // others run are admitted as soon as a slot frees.  A host callback at the end of each batch
 // wakes the scheduler, which scatters the results into the requests' output buffers and
-// completes the requests whose pieces are all done.
+// completes the requests whose pieces are all done.  Each slot has its own completion thread,
+// which copies its batch's results out of pinned memory into the requests' buffers outside the
+// server lock, so the copies of different slots run in parallel and never hold up the scheduler.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -74,6 +76,10 @@ struct Slot {
     std::vector<uint64_t> piece_win;  // first window of each piece inside the batch output
     bool busy = false;
     std::atomic<bool> complete{false};
+    // completion thread: woken by the batch's host callback
+    std::thread finisher;
+    std::mutex fmu;
+    std::condition_variable fcv;
     ~Slot() {
         if (graph) cudaGraphExecDestroy(graph);
         if (h_ascii) cudaFreeHost(h_ascii);
@@ -118,6 +124,8 @@ struct scb_server {
     bool have_first = false;
 
     void run();
+    void finish(Slot& s);
+    std::atomic<bool> stop_finishers{false};
     void add_spectrum(TileArgs& d, unsigned int* tile_counter) const;
     scb_status clear_spectrum(cudaStream_t st);
     scb_status launch(Slot& s);
@@ -134,7 +142,7 @@ namespace {
 void CUDART_CB on_batch_done(void* p) {
     auto* pair = static_cast<std::pair<scb_server*, Slot*>*>(p);
     pair->second->complete.store(true, std::memory_order_release);
-    pair->first->wake.notify_one();
+    pair->second->fcv.notify_one();
     delete pair;
 }
 
@@ -303,15 +311,41 @@ scb_status scb_server::launch(Slot& s) {
     return SCB_OK;
 }
 
+// The slot's completion thread: waits for its batch's host callback (polling every 100 us, so a
+// notification that arrives before the wait is never lost for long), copies the results into the
+// requests' buffers without the server lock (a request's buffers stay valid until its wait returns,
+// which needs this batch), then completes the pieces under the lock.
+void scb_server::finish(Slot& s) {
+    cudaSetDevice(ctx->device);
+    while (true) {
+        {
+            std::unique_lock<std::mutex> lk(s.fmu);
+            s.fcv.wait_for(lk, std::chrono::microseconds(100),
+                           [&] { return s.complete.load(std::memory_order_acquire) || stop_finishers.load(); });
+        }
+        if (!s.complete.load(std::memory_order_acquire)) {
+            if (stop_finishers.load()) break;
+            continue;
+        }
+        for (size_t i = 0; i < s.pieces.size(); i++) {
+            const Piece& p = s.pieces[i];
+            if (p.windows) {
+                std::memcpy(p.req->out + p.win0, s.h_out + s.piece_win[i], p.windows * 8);
+                std::memcpy(p.req->valid + p.win0, s.h_outv + s.piece_win[i], p.windows);
+            }
+        }
+        std::lock_guard<std::mutex> lk(mu);
+        s.complete.store(false, std::memory_order_relaxed);
+        complete(s);
+        wake.notify_one();
+    }
+}
+
 void scb_server::complete(Slot& s) {
     const auto now = Clock::now();
     for (size_t i = 0; i < s.pieces.size(); i++) {
         const Piece& p = s.pieces[i];
         Request& r = *p.req;
-        if (p.windows) {
-            std::memcpy(r.out + p.win0, s.h_out + s.piece_win[i], p.windows * 8);
-            std::memcpy(r.valid + p.win0, s.h_outv + s.piece_win[i], p.windows);
-        }
         if (--r.pieces_left == 0) {
             r.done = true;
             r.finish = now;
@@ -329,9 +363,6 @@ void scb_server::run() {
     cudaSetDevice(ctx->device);
     std::unique_lock<std::mutex> lk(mu);
     while (true) {
-        for (auto& sp : slots) {
-            if (sp->busy && sp->complete.load(std::memory_order_acquire)) complete(*sp);
-        }
         if (stop && pending.empty()) {
             bool idle = true;
             for (auto& sp : slots) idle = idle && !sp->busy;
@@ -369,12 +400,9 @@ void scb_server::run() {
                 settled.notify_all();
             }
         }
-        bool free_slot = false;
-        for (auto& sp : slots) free_slot = free_slot || !sp->busy;
         wake.wait_for(lk, std::chrono::microseconds(100), [&] {
-            for (auto& sp : slots) {
-                if (sp->busy && sp->complete.load(std::memory_order_acquire)) return true;
-            }
+            bool free_slot = false;
+            for (auto& sp : slots) free_slot = free_slot || !sp->busy;
             return (free_slot && !pending.empty()) || (stop && pending.empty());
         });
     }
@@ -444,6 +472,10 @@ scb_status scb_server_create(scb_ctx* ctx, const scb_server_config* cfg_in, scb_
         SCB_TRY(srv->clear_spectrum(srv->slots[0]->stream));
     }
     scb_server* raw = srv.release();
+    for (auto& sp : raw->slots) {
+        Slot* s = sp.get();
+        s->finisher = std::thread([raw, s] { raw->finish(*s); });
+    }
     raw->worker = std::thread([raw] { raw->run(); });
     *out = raw;
     return SCB_OK;
@@ -636,9 +668,14 @@ void scb_server_destroy(scb_server* s) {
         s->stop = true;
     }
     s->wake.notify_all();
-    if (s->worker.joinable()) s->worker.join();
+    if (s->worker.joinable()) s->worker.join();  // returns once every slot is idle
     cudaSetDevice(s->ctx->device);
     for (auto& sp : s->slots) cudaStreamSynchronize(sp->stream);
+    s->stop_finishers.store(true);
+    for (auto& sp : s->slots) {
+        sp->fcv.notify_all();
+        if (sp->finisher.joinable()) sp->finisher.join();
+    }
     delete s;
 }
 
