@@ -65,7 +65,7 @@ struct Piece {
 struct Slot {
     cudaStream_t stream = nullptr;
     DevBuf ascii, offsets, woff, codes, valid, seqstart, out, outv, cnt, tiles, params;
-    cudaGraphExec_t graph = nullptr;  // the slot's batch, captured at its first batch
+    cudaGraphExec_t graph = nullptr;  // the slot's batch, captured when the server starts
     uint64_t graph_launches = 0;
     uint8_t* h_ascii = nullptr;
     uint64_t* h_offsets = nullptr;
@@ -470,6 +470,11 @@ scb_status scb_server_create(scb_ctx* ctx, const scb_server_config* cfg_in, scb_
         SCB_TRY(srv->spec_ovf.ensure(srv->spec_ovf_cap * 8));
         SCB_TRY(srv->spec_cnt.ensure(kCntSlots * 8));
         SCB_TRY(srv->clear_spectrum(srv->slots[0]->stream));
+    }
+    // every slot's graph is captured here, before the first request: a slot that first runs while
+    // others are busy (the first burst of arrivals) would otherwise hold its batch behind a capture
+    if (srv->use_graphs) {
+        for (auto& sp : srv->slots) SCB_TRY(srv->capture(*sp));
     }
     scb_server* raw = srv.release();
     for (auto& sp : raw->slots) {
