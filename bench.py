@@ -63,6 +63,10 @@ def parse():
                    help="run one insert + query of a small case (for ncu) and exit")
     p.add_argument("--profile-scale", type=float, default=0.1,
                    help="genome scale of the profile case (1.0 = the full 2 Gbp workload)")
+    p.add_argument("--profile-slots", type=int, default=GEOM["counter_slots_exponent"],
+                   help="counter_slots_exponent of the profile case: scale 0.25 with 2^28 slots keeps the full "
+                        "workload's records per block, so its buckets (4 blocks, about 500 records) are the full "
+                        "run's")
     return p.parse_args()
 
 
@@ -934,9 +938,10 @@ def run_mixed(args, dist: Dist) -> dict:
 
 
 def run_profile_case(args):
-    """One insert + one stream query with the chosen strategy, on the 2 GiB table: genome scale
-    0.1 (200 MB of reads) for multi-pass ncu captures, scale 1.0 (the full 2 Gbp) for one-pass
-    DRAM-byte captures."""
+    """One insert + one stream query with the chosen strategy, for ncu: by default genome scale 0.1
+    (200 MB of reads) on the 2 GiB table; with --profile-scale 0.25 --profile-slots 28 (500 MB of
+    reads, a 512 MiB table) the workload has the full run's records per block and bucket, so its
+    per-unit instruction and DRAM figures scale to the full 2 Gbp step by the units processed."""
     import torch
 
     from scbf_b200 import _lib, api
@@ -945,7 +950,7 @@ def run_profile_case(args):
     data, offsets = workload(0, args.profile_scale)
     cfg = api.SuperCountingBloomConfig(k=GEOM["k"], m=GEOM["m"], s=GEOM["s"], n_hashes=GEOM["n_hashes"],
                                        counter_bits=api.CounterBits(GEOM["counter_bits"]),
-                                       counter_slots_exponent=GEOM["counter_slots_exponent"],
+                                       counter_slots_exponent=args.profile_slots,
                                        block_slots_exponent=GEOM["block_slots_exponent"], threads=1, queue=4096)
     ctx = api._create(cfg)
     sid = STRATEGY_IDS[args.profile_case]

@@ -364,8 +364,12 @@ void attach_deferred(const Lane& L, GroupArgs& ga) {
     ga.item_base = L.ditem_base.as<unsigned long long>();
 }
 
-uint64_t probe_capacity(const scb_ctx* ctx, uint64_t n_bytes) {
-    return n_bytes + records_estimate(ctx, n_bytes) * (ctx->g.k - ctx->g.s);
+// In a build apply only the items it leaves to the query kernel (split buckets, items with more
+// s-mers than the kept region) store probe words, a few percent of the s-mers: an eighth of the
+// capacity suffices there (items past it hash again), which keeps 25 GB off the device at 2 Gbp.
+uint64_t probe_capacity(const scb_ctx* ctx, uint64_t n_bytes, bool build) {
+    const uint64_t all = n_bytes + records_estimate(ctx, n_bytes) * (ctx->g.k - ctx->g.s);
+    return build ? all / 8 + 65536 : all;
 }
 
 // Turns on probe reuse in the apply arguments: the insert writes (and first clears the count),
@@ -545,7 +549,7 @@ scb_status grouped_prepare(scb_ctx* ctx, Lane& L, TileArgs& a, cudaStream_t st) 
     gs.probes_written = false;
     gs.probe_cap = 0;
     if (L.want_probes && records) {
-        gs.probe_cap = probe_capacity(ctx, a.n_bytes);
+        gs.probe_cap = probe_capacity(ctx, a.n_bytes, L.want_build);
         SCB_TRY(L.probes.ensure(gs.probe_cap * 8));
         SCB_TRY(L.item_base.ensure(z.max_items * 8));
     }
@@ -855,7 +859,7 @@ scb_status graph_launch(scb_ctx* ctx, Lane& L, int kind, const uint8_t* d_ascii,
                               (kind == kBatchBuildStream && K.s_ins == SCB_STRATEGY_GROUPED &&
                                K.s_query == SCB_STRATEGY_GROUPED);
             if (keep && probes_fit(ctx)) {
-                K.probe_cap = probe_capacity(ctx, cls);
+                K.probe_cap = probe_capacity(ctx, cls, K.fused);
                 SCB_TRY(L.probes.ensure(K.probe_cap * 8));
                 SCB_TRY(L.item_base.ensure(z.max_items * 8));
             }

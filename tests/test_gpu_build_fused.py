@@ -114,3 +114,19 @@ def test_fused_build_equals_two_pass_on_short_reads(scb):
     two = _build_stream(scb, geom, 16, data, offsets, fused=False)
     assert fused[0] == two[0] and fused[1] == two[1]
     assert np.array_equal(fused[2], two[2])
+
+
+def test_fused_build_large_exclusive_items_are_deferred_and_exact(scb, oracle_mod):
+    """A table of eight blocks: most buckets' only work item holds about 3 000 records (35 000
+    s-mers), more probe words than a CTA keeps, so it stores them in item order for the
+    query-only pass; the counts, report and table stay the oracle's."""
+    from scbf_b200 import workloads
+
+    data, offsets = workloads.short_reads(genome_len=100_000, n_reads=1200, read_len=150, seed=8, sub_rate=0.01,
+                                          n_rate=0.0)
+    geom = (31, 21, 25, 4, 12, 9)
+    ref = _oracle(oracle_mod, geom, 16, data, offsets)
+    for graphs in (True, False):
+        got = _build_stream(scb, geom, 16, data, offsets, graphs=graphs)
+        assert got[0] == ref[0] and got[1] == ref[1], graphs
+        assert np.array_equal(got[2], ref[2])
