@@ -418,20 +418,38 @@ def run_ours(args, dist: Dist):
     if not args.no_e2e:
         p_data = torch.from_numpy(data).pin_memory()
         p_off = torch.from_numpy(offsets.view(np.int64)).pin_memory()
-        times = []
-        for i in range(args.warmup + args.steps):
-            check(L.scb_reset(h))
-            torch.cuda.synchronize()
-            dist.barrier()
-            t0 = time.perf_counter()
-            check(L.scb_build_and_stream_query(h, p_data.data_ptr(), p_off.data_ptr(), n_seqs, C.byref(km),
-                                               C.byref(sm), C.byref(rep)))
-            dt = time.perf_counter() - t0
-            if i >= args.warmup:
-                times.append(dist.max(dt))
-        assert (rep.valid_kmers, rep.positive_estimates, rep.estimate_checksum) == reference_report
-        e2e = {"value": all_kmers * len(times) / sum(times), "unit": "k-mers/s",
-               "h2d_bytes_per_step": n_bytes + (n_seqs + 1) * 8, "d2h_bytes_per_step": 2 * (16 * 8 + 4) + 8}
+        h2d = C.c_uint64(0)
+
+        def e2e_steps():
+            """Timed steps through the host entry point; returns (k-mers/s, bytes copied last step)."""
+            times = []
+            h2d_before = 0
+            for i in range(args.warmup + args.steps):
+                check(L.scb_reset(h))
+                torch.cuda.synchronize()
+                dist.barrier()
+                check(L.scb_h2d_bytes(h, C.byref(h2d)))
+                h2d_before = h2d.value
+                t0 = time.perf_counter()
+                check(L.scb_build_and_stream_query(h, p_data.data_ptr(), p_off.data_ptr(), n_seqs, C.byref(km),
+                                                   C.byref(sm), C.byref(rep)))
+                dt = time.perf_counter() - t0
+                if i >= args.warmup:
+                    times.append(dist.max(dt))
+            assert (rep.valid_kmers, rep.positive_estimates, rep.estimate_checksum) == reference_report
+            check(L.scb_h2d_bytes(h, C.byref(h2d)))
+            return all_kmers * len(times) / sum(times), h2d.value - h2d_before
+
+        # the letters copied and packed on the device, for comparison; then the default: the reads
+        # packed on the host (3 bits per base) while the GPU works on the previous piece
+        check(L.scb_set_host_pack(h, 0))
+        letters_value, letters_h2d = e2e_steps()
+        check(L.scb_set_host_pack(h, 1))
+        e2e_value, e2e_h2d = e2e_steps()
+        # h2d: the library's own count of the bytes it copied in the last step
+        e2e = {"value": e2e_value, "unit": "k-mers/s", "h2d_bytes_per_step": e2e_h2d,
+               "d2h_bytes_per_step": 2 * (16 * 8 + 4) + 8, "host_input_bytes_per_step": n_bytes + (n_seqs + 1) * 8,
+               "without_host_pack": {"value": letters_value, "h2d_bytes_per_step": letters_h2d}}
 
     # roofline of the dominant kernel of the timed step.  Algorithmic bytes follow the design the
     # kernel implements: the grouped kernels stage each touched counter block once per bucket, so

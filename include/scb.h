@@ -255,6 +255,17 @@ scb_status scb_set_fused_build(scb_ctx* ctx, int enable);
  * the grouped strategy; results are identical to one batch. */
 scb_status scb_set_piece_bytes(scb_ctx* ctx, uint64_t piece_bytes);
 
+/* Host packing of those pieces (performance setting, no reference counterpart; on by default):
+ * the host packs each piece into the device's 2-bit code and validity layout on all host
+ * threads, into pinned staging, and copies 3 bits per base instead of the 8-bit letters; piece
+ * p + 1 is packed while the GPU works on piece p.  enable = 0 copies the letters and packs on the
+ * device.  Results are identical either way. */
+scb_status scb_set_host_pack(scb_ctx* ctx, int enable);
+
+/* Bytes the host entry points of this context have copied to the device since it was created
+ * (sequences or their packed form, offsets); no reference counterpart, a measurement aid. */
+scb_status scb_h2d_bytes(scb_ctx* ctx, uint64_t* bytes);
+
 /* Host FASTA/FASTQ reader (replaces the reference's parser thread feeding the workers,
  * src/api.rs:621-674, with its record rules, src/api.rs:893-915): reads a plain or gzip file in
  * one pass into concatenated sequences with n_records + 1 offsets (the layout of

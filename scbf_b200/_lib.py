@@ -139,6 +139,8 @@ def load(path: str | None = None):
         "scb_get_timings": (C.c_int, [ctxp, C.POINTER(ScbTimings)]),
         "scb_set_graphs": (C.c_int, [ctxp, C.c_int]),
         "scb_set_piece_bytes": (C.c_int, [ctxp, C.c_uint64]),
+        "scb_set_host_pack": (C.c_int, [ctxp, C.c_int]),
+        "scb_h2d_bytes": (C.c_int, [ctxp, C.POINTER(C.c_uint64)]),
         "scb_set_fused_build": (C.c_int, [ctxp, C.c_int]),
         "scb_fastx_read": (C.c_int, [C.c_char_p, C.POINTER(vp)]),
         "scb_fastx_sequences": (C.c_int, [vp, C.POINTER(vp), C.POINTER(vp), u64p]),

@@ -225,10 +225,12 @@ scb_status prepare_batch(scb_ctx* ctx, Lane& L, const uint8_t* d_ascii, const ui
     const uint64_t groups = (n_bytes + 31) / 32;
     L.gs.valid = false;
     SCB_TRY(mark(ctx, L, 0, st));
-    SCB_CUDA(cudaMemsetAsync(L.codes.p, 0, (2 * groups + kPadWords) * 4, st));
-    SCB_CUDA(cudaMemsetAsync(L.valid.p, 0, (groups + kPadWords) * 4, st));
+    if (!L.prepacked) {  // a prepacked lane's codes and bitmap hold the batch already
+        SCB_CUDA(cudaMemsetAsync(L.codes.p, 0, (2 * groups + kPadWords) * 4, st));
+        SCB_CUDA(cudaMemsetAsync(L.valid.p, 0, (groups + kPadWords) * 4, st));
+        launch_pack(d_ascii, n_bytes, L.codes.as<uint32_t>(), L.valid.as<uint32_t>(), st);
+    }
     SCB_CUDA(cudaMemsetAsync(L.seqstart.p, 0, (groups + kPadWords) * 4, st));
-    launch_pack(d_ascii, n_bytes, L.codes.as<uint32_t>(), L.valid.as<uint32_t>(), st);
     launch_seqstart(d_offsets, n_seqs, n_bytes, L.seqstart.as<uint32_t>(), st);
     SCB_TRY(mark(ctx, L, 1, st));
     if (ctx->timing) L.spans |= kSpanPack;
@@ -695,7 +697,7 @@ scb_status record_batch(scb_ctx* ctx, Lane& L, const GraphKey& K, cudaStream_t s
     if (K.kind != kBatchReportKept) {  // a kept batch's codes are still in the lane
         SCB_TRY(mark(ctx, L, 0, st));
         launch_clear_dyn(bp, L.seqstart.as<uint32_t>(), nullptr, nullptr, sms, st);
-        launch_pack_dyn(bp, L.codes.as<uint32_t>(), L.valid.as<uint32_t>(), sms, st);
+        if (!K.prepacked) launch_pack_dyn(bp, L.codes.as<uint32_t>(), L.valid.as<uint32_t>(), sms, st);
         launch_seqstart_dyn(bp, L.seqstart.as<uint32_t>(), sms, st);
         SCB_TRY(mark(ctx, L, 1, st));
         SCB_CUDA(cudaMemsetAsync(L.cnt.p, 0, kCntSlots * 8, st));
@@ -831,6 +833,7 @@ scb_status graph_launch(scb_ctx* ctx, Lane& L, int kind, const uint8_t* d_ascii,
     } else {
         if (!ctx->graphs) return SCB_OK;
         K.kind = kind;
+        K.prepacked = L.prepacked;
         if (kind_inserts(kind)) K.s_ins = resolve(ctx, ctx->insert_strategy, n_bytes, true);
         if (kind_queries(kind)) K.s_query = resolve(ctx, ctx->query_strategy, n_bytes, false);
         if (K.s_ins == SCB_STRATEGY_PLAIN || K.s_query == SCB_STRATEGY_PLAIN) return SCB_OK;
@@ -1019,6 +1022,7 @@ scb_status upload_chunk(scb_ctx* ctx, Lane& L, const uint8_t* seqs, const uint64
     cudaStream_t st = L.stream;
     if (n_bytes) SCB_CUDA(cudaMemcpyAsync(L.ascii.p, seqs + c.byte0, n_bytes, cudaMemcpyHostToDevice, st));
     SCB_CUDA(cudaMemcpyAsync(L.offsets.p, offsets + c.seq0, (n_seqs + 1) * 8, cudaMemcpyHostToDevice, st));
+    ctx->h2d_bytes += n_bytes + (n_seqs + 1) * 8;
     if (c.byte0) {
         k_rebase<<<(unsigned)((n_seqs + 1 + 255) / 256), 256, 0, st>>>(L.offsets.as<uint64_t>(), n_seqs + 1, c.byte0);
         note_launch();
@@ -1432,6 +1436,7 @@ static bool pieces_apply(const scb_ctx* ctx, uint64_t total) {
 static scb_status preload_first_piece(scb_ctx* ctx, const uint8_t* seqs, const uint64_t* offsets, uint64_t n,
                                       uint64_t& pre) {
     pre = 0;
+    if (ctx->host_pack) return SCB_OK;  // the pieces are packed on the host first
     if (!seqs || !n || offsets[n] < offsets[0] || !pieces_apply(ctx, offsets[n] - offsets[0])) return SCB_OK;
     const uint64_t first = (uint64_t)ramp_first(piece_bytes_for(ctx, offsets[n] - offsets[0]));
     if (!first || first >= offsets[n] - offsets[0]) return SCB_OK;
@@ -1439,9 +1444,41 @@ static scb_status preload_first_piece(scb_ctx* ctx, const uint8_t* seqs, const u
     Lane& L = *ctx->piece_lanes[0];
     SCB_TRY(L.ascii.ensure((first + 31) / 32 * 32 + 64));
     SCB_CUDA(cudaMemcpyAsync(L.ascii.p, seqs + offsets[0], first, cudaMemcpyHostToDevice, ctx->copy_stream));
+    ctx->h2d_bytes += first;
     pre = first;
     return SCB_OK;
 }
+
+// Pinned staging for host-packed pieces of up to `groups` 32-byte groups: two areas, so the host
+// packs piece p + 1 while piece p's copy reads the other.
+static scb_status ensure_staging(scb_ctx* ctx, uint64_t groups) {
+    for (int i = 0; i < 2; i++) {
+        if (!ctx->stage_free[i]) SCB_CUDA(cudaEventCreateWithFlags(&ctx->stage_free[i], cudaEventDisableTiming));
+    }
+    if (groups <= ctx->stage_groups) return SCB_OK;
+    SCB_CUDA(cudaStreamSynchronize(ctx->copy_stream));
+    for (int i = 0; i < 2; i++) {
+        if (ctx->stage_codes[i]) cudaFreeHost(ctx->stage_codes[i]);
+        if (ctx->stage_valid[i]) cudaFreeHost(ctx->stage_valid[i]);
+        ctx->stage_codes[i] = nullptr;
+        ctx->stage_valid[i] = nullptr;
+    }
+    ctx->stage_groups = 0;
+    for (int i = 0; i < 2; i++) {
+        SCB_CUDA(cudaMallocHost((void**)&ctx->stage_codes[i], (2 * groups + kPadWords) * 4));
+        SCB_CUDA(cudaMallocHost((void**)&ctx->stage_valid[i], (groups + kPadWords) * 4));
+    }
+    ctx->stage_groups = groups;
+    return SCB_OK;
+}
+
+// Clears the prepacked mark of the piece lanes when a host build + stream query leaves.
+struct PrepackedReset {
+    scb_ctx* ctx;
+    ~PrepackedReset() {
+        for (auto& pl : ctx->piece_lanes) pl->prepacked = false;
+    }
+};
 
 // Host build + stream query of a large batch in pieces, each in its own lane: piece p + 1 is
 // copied to the device on the copy stream while piece p's insert graph runs, every piece keeps
@@ -1474,13 +1511,43 @@ static scb_status build_stream_pieces(scb_ctx* ctx, const uint8_t* seqs, const u
     // overlaps the GPU's work on the pieces already launched.  The first piece's bytes are already
     // on their way when it fits the preloaded size (a longer first sequence reallocates the
     // buffer, after the copy, and copies the piece again).
+    // With host packing (the default) the host packs each piece into the device layout in a pinned
+    // staging area (all host threads) and copies 3 bits per base instead of the 8-bit letters; it
+    // packs piece p + 1 while the GPU works on piece p.
+    const bool hp = ctx->host_pack;
+    PrepackedReset reset_marks{ctx};
+    if (hp) {
+        uint64_t max_groups = 0;
+        for (const Chunk& c : pieces) max_groups = std::max<uint64_t>(max_groups, (c.byte1 - c.byte0 + 31) / 32);
+        SCB_TRY(ensure_staging(ctx, max_groups));
+    }
+    const unsigned pack_threads = std::max(1u, std::thread::hardware_concurrency());
     auto upload = [&](size_t p) -> scb_status {
         const Chunk& c = pieces[p];
         Lane& L = *ctx->piece_lanes[p];
         const uint64_t ns = c.seq1 - c.seq0, nb = c.byte1 - c.byte0;
         SCB_TRY(ensure_lane(ctx, L, nb, ns));
-        if (p != 0 || nb > pre) SCB_CUDA(cudaMemcpyAsync(L.ascii.p, seqs + c.byte0, nb, cudaMemcpyHostToDevice, xs));
+        if (hp) {
+            // the piece's graph sizes the lane's work buffers for its byte class: grow them before
+            // the copy, so that no later growth drops the copied codes
+            SCB_TRY(ensure_lane_work(ctx, L, std::max(nb, std::min(class_bytes(nb), kMaxBatchBytes - 64))));
+            const uint64_t groups = (nb + 31) / 32;
+            const int s = (int)(p & 1);
+            SCB_CUDA(cudaEventSynchronize(ctx->stage_free[s]));  // the copy that last read this area
+            host_pack(seqs + c.byte0, nb, ctx->stage_codes[s], ctx->stage_valid[s], pack_threads);
+            SCB_CUDA(cudaMemcpyAsync(L.codes.p, ctx->stage_codes[s], (2 * groups + kPadWords) * 4,
+                                     cudaMemcpyHostToDevice, xs));
+            SCB_CUDA(cudaMemcpyAsync(L.valid.p, ctx->stage_valid[s], (groups + kPadWords) * 4, cudaMemcpyHostToDevice,
+                                     xs));
+            SCB_CUDA(cudaEventRecord(ctx->stage_free[s], xs));
+            ctx->h2d_bytes += (3 * groups + 2 * kPadWords) * 4;
+            L.prepacked = true;
+        } else if (p != 0 || nb > pre) {
+            SCB_CUDA(cudaMemcpyAsync(L.ascii.p, seqs + c.byte0, nb, cudaMemcpyHostToDevice, xs));
+            ctx->h2d_bytes += nb;
+        }
         SCB_CUDA(cudaMemcpyAsync(L.offsets.p, offsets + c.seq0, (ns + 1) * 8, cudaMemcpyHostToDevice, xs));
+        ctx->h2d_bytes += (ns + 1) * 8;
         SCB_CUDA(cudaEventRecord(ctx->piece_events[p], xs));
         return SCB_OK;
     };
@@ -1836,6 +1903,20 @@ scb_status scb_set_piece_bytes(scb_ctx* ctx, uint64_t piece_bytes) {
     if (!ctx) return fail_kind(SCB_ERR_INTERNAL_STATE, "null context");
     CtxLock lk(ctx);
     ctx->piece_bytes = piece_bytes;
+    return SCB_OK;
+}
+
+scb_status scb_set_host_pack(scb_ctx* ctx, int enable) {
+    if (!ctx) return fail_kind(SCB_ERR_INTERNAL_STATE, "null context");
+    CtxLock lk(ctx);
+    ctx->host_pack = enable != 0;
+    return SCB_OK;
+}
+
+scb_status scb_h2d_bytes(scb_ctx* ctx, uint64_t* bytes) {
+    if (!ctx || !bytes) return fail_kind(SCB_ERR_INTERNAL_STATE, "null argument");
+    CtxLock lk(ctx);
+    *bytes = ctx->h2d_bytes;
     return SCB_OK;
 }
 

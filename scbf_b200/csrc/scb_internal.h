@@ -141,9 +141,11 @@ struct GraphKey {
     uint64_t cap_bytes = 0, rec_cap = 0, bucket_cap = 0, max_items = 0, n_buckets = 0, probe_cap = 0;
     uint32_t shift = 0, apply_threads = 0;
     bool fused = false;  // a grouped build + stream query in one build apply (plus deferred items)
+    bool prepacked = false;  // the batch's codes and bitmap came packed from the host
     uint64_t sig = 0;
     bool operator==(const GraphKey& o) const {
         return kind == o.kind && s_ins == o.s_ins && s_query == o.s_query && fused == o.fused &&
+               prepacked == o.prepacked &&
                cap_bytes == o.cap_bytes && rec_cap == o.rec_cap && bucket_cap == o.bucket_cap &&
                probe_cap == o.probe_cap &&
                max_items == o.max_items && n_buckets == o.n_buckets && shift == o.shift &&
@@ -173,6 +175,9 @@ struct Lane {
     bool want_probes = false;
     bool want_build = false;  // the grouped insert of this batch is a build apply
     bool want_spectrum = false;  // buckets sized for the spectrum apply
+    // codes and valid hold the batch already (packed on the host and copied), so the batch skips
+    // the device packing kernel
+    bool prepacked = false;
     cudaStream_t stream = nullptr;
     GroupedState gs;
     cudaEvent_t ev[kLaneEvents] = {};
@@ -208,6 +213,11 @@ struct Tuning {
     uint64_t host_batch_bytes = kMaxBatchBytes - 64;  // sequence bytes per batch of a host call
 };
 
+// Packs n sequence bytes on the host into the device layout of kernel (a) (codes: 16 bases per
+// 32-bit word; valid: 32 bases per word; kPadWords zero words after each), on up to `threads`
+// threads (scb_hostpack.cpp).
+void host_pack(const uint8_t* ascii, uint64_t n, uint32_t* codes, uint32_t* valid, unsigned threads);
+
 }  // namespace scb
 
 struct scb_ctx {
@@ -232,12 +242,26 @@ struct scb_ctx {
     cudaStream_t copy_stream = nullptr;
     std::vector<cudaEvent_t> piece_events;
     uint64_t piece_bytes = 0;  // 0: the default
+    // host packing of the pieces (scb_set_host_pack): two pinned staging areas, each the codes and
+    // valid words of the largest piece, reused once the copy that read them (stage_free) is done
+    bool host_pack = true;
+    uint32_t* stage_codes[2] = {nullptr, nullptr};
+    uint32_t* stage_valid[2] = {nullptr, nullptr};
+    uint64_t stage_groups = 0;
+    cudaEvent_t stage_free[2] = {nullptr, nullptr};
+    uint64_t h2d_bytes = 0;  // bytes the host entry points copied to the device (scb_h2d_bytes)
     bool timing = false;
     bool graphs = true;  // replay batches through graphs captured per shape class
     bool fused_build = true;  // a grouped build + stream query answers exclusive buckets in its insert
     scb_timings times{};
     std::mutex mu;
     ~scb_ctx() {
+        if (copy_stream) cudaStreamSynchronize(copy_stream);
+        for (int i = 0; i < 2; i++) {
+            if (stage_codes[i]) cudaFreeHost(stage_codes[i]);
+            if (stage_valid[i]) cudaFreeHost(stage_valid[i]);
+            if (stage_free[i]) cudaEventDestroy(stage_free[i]);
+        }
         for (auto e : piece_events) cudaEventDestroy(e);
         if (copy_stream) cudaStreamDestroy(copy_stream);
         piece_lanes.clear();

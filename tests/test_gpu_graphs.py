@@ -205,12 +205,16 @@ def test_build_and_stream_probe_slots_overflow(scb, oracle_mod, graphs):
     ctx.close()
 
 
-@pytest.mark.parametrize("pinned,long_first", [(False, False), (True, False), (True, True)])
-def test_host_build_and_stream_in_pieces_matches_oracle(scb, oracle_mod, pinned, long_first):
+@pytest.mark.parametrize("pinned,long_first,host_pack", [(False, False, True), (True, False, True),
+                                                          (True, True, True), (False, False, False),
+                                                          (True, True, False)])
+def test_host_build_and_stream_in_pieces_matches_oracle(scb, oracle_mod, pinned, long_first, host_pack):
     """The host build + stream query split into pieces (copy of piece p + 1 overlapping the insert
     of piece p, each piece queried on its kept records after the last insert) gives exactly the
-    oracle's counts, report and table, from pageable or pinned host memory, also when the first
-    sequence is longer than the first piece's bytes copied while the offsets are validated."""
+    oracle's counts, report and table, from pageable or pinned host memory, with the pieces packed
+    on the host (3 bits per base copied) or packed on the device from copied letters, also when
+    the first sequence is longer than the first piece's bytes copied while the offsets are
+    validated.  The bytes copied are the packed layout's, or the letters', plus the offsets."""
     import torch
 
     from scbf_b200 import _lib, api
@@ -235,12 +239,23 @@ def test_host_build_and_stream_in_pieces_matches_oracle(scb, oracle_mod, pinned,
     ctx = api._create(cfg)
     assert L.scb_set_strategy(ctx.h, _lib.STRATEGIES["grouped"], _lib.STRATEGIES["grouped"]) == 0
     assert L.scb_set_piece_bytes(ctx.h, 1 << 20) == 0  # pieces of 0.45 MiB growing to 1 MiB: about eight
+    assert L.scb_set_host_pack(ctx.h, 1 if host_pack else 0) == 0
     km, sm = C.c_uint64(), C.c_uint64()
     rep = _lib.ScbReport()
+    n_bytes, n_seqs = int(offsets[-1]), len(offsets) - 1
     for _ in range(2):
         assert L.scb_reset(ctx.h) == 0
+        b0, b1 = C.c_uint64(), C.c_uint64()
+        assert L.scb_h2d_bytes(ctx.h, C.byref(b0)) == 0
         assert L.scb_build_and_stream_query(ctx.h, dp, op, len(offsets) - 1, C.byref(km), C.byref(sm),
                                             C.byref(rep)) == 0, _lib.last_error()
+        assert L.scb_h2d_bytes(ctx.h, C.byref(b1)) == 0
+        copied = b1.value - b0.value
+        if host_pack:  # 3 bits per base plus padding per piece, and the offsets of every piece
+            assert n_bytes * 3 // 8 < copied < n_bytes * 3 // 8 + 20 * 256 + (n_seqs + 20) * 8
+        else:
+            # (a first sequence longer than the preloaded first piece copies that piece again)
+            assert n_bytes + (n_seqs + 1) * 8 <= copied <= n_bytes + (1 << 20) + (n_seqs + 20) * 8
         assert (km.value, sm.value) == (okm, osm)
         assert (rep.records_processed, rep.total_windows, rep.valid_kmers, rep.positive_estimates,
                 rep.estimate_checksum) == (oq.records_processed, oq.total_windows, oq.valid_kmers,
