@@ -1015,14 +1015,74 @@ scb_status run_batch(scb_ctx* ctx, Lane& L, int kind, const uint8_t* d_ascii, co
     return SCB_OK;
 }
 
-// Copies a host chunk into the lane and rebases its offsets.
+// Pinned staging for host packing of up to `groups` 32-byte groups: two areas, so the host packs
+// piece (or slice) p + 1 while the copy of piece p reads the other.
+static scb_status ensure_staging(scb_ctx* ctx, uint64_t groups) {
+    for (int i = 0; i < 2; i++) {
+        if (!ctx->stage_free[i]) SCB_CUDA(cudaEventCreateWithFlags(&ctx->stage_free[i], cudaEventDisableTiming));
+    }
+    if (groups <= ctx->stage_groups) return SCB_OK;
+    for (int i = 0; i < 2; i++) SCB_CUDA(cudaEventSynchronize(ctx->stage_free[i]));  // copies still reading
+    for (int i = 0; i < 2; i++) {
+        if (ctx->stage_codes[i]) cudaFreeHost(ctx->stage_codes[i]);
+        if (ctx->stage_valid[i]) cudaFreeHost(ctx->stage_valid[i]);
+        ctx->stage_codes[i] = nullptr;
+        ctx->stage_valid[i] = nullptr;
+    }
+    ctx->stage_groups = 0;
+    for (int i = 0; i < 2; i++) {
+        SCB_CUDA(cudaMallocHost((void**)&ctx->stage_codes[i], (2 * groups + kPadWords) * 4));
+        SCB_CUDA(cudaMallocHost((void**)&ctx->stage_valid[i], (groups + kPadWords) * 4));
+    }
+    ctx->stage_groups = groups;
+    return SCB_OK;
+}
+
+// Host packing of one upload: slices of kPackSlice bytes are packed on all host threads into the
+// two staging areas in turn and copied to their place in the lane's codes and validity words (the
+// padding words with the last slice), so slice i + 1 is packed while slice i copies.
+constexpr uint64_t kPackSlice = 256ull << 20;  // a multiple of 32: slices end on whole groups
+constexpr uint64_t kHostPackMin = 1ull << 20;  // smaller uploads copy the letters
+scb_status host_pack_upload(scb_ctx* ctx, Lane& L, const uint8_t* src, uint64_t n_bytes, cudaStream_t st) {
+    SCB_TRY(ensure_staging(ctx, (std::min(n_bytes, kPackSlice) + 31) / 32));
+    const unsigned threads = std::max(1u, std::thread::hardware_concurrency());
+    uint32_t* codes = L.codes.as<uint32_t>();
+    uint32_t* valid = L.valid.as<uint32_t>();
+    for (uint64_t off = 0, i = 0; off < n_bytes; off += kPackSlice, i++) {
+        const uint64_t len = std::min(kPackSlice, n_bytes - off), g = (len + 31) / 32;
+        const uint64_t pad = off + len == n_bytes ? kPadWords : 0;
+        const int s = (int)(i & 1);
+        SCB_CUDA(cudaEventSynchronize(ctx->stage_free[s]));  // the copy that last read this area
+        host_pack(src + off, len, ctx->stage_codes[s], ctx->stage_valid[s], threads);
+        SCB_CUDA(cudaMemcpyAsync(codes + off / 16, ctx->stage_codes[s], (2 * g + pad) * 4, cudaMemcpyHostToDevice, st));
+        SCB_CUDA(cudaMemcpyAsync(valid + off / 32, ctx->stage_valid[s], (g + pad) * 4, cudaMemcpyHostToDevice, st));
+        SCB_CUDA(cudaEventRecord(ctx->stage_free[s], st));
+        ctx->h2d_bytes += (3 * g + 2 * pad) * 4;
+    }
+    return SCB_OK;
+}
+
+// Copies a host chunk into the lane and rebases its offsets.  Uploads of at least kHostPackMin
+// bytes are packed on the host (3 bits per base cross PCIe, and pageable input needs no driver
+// staging of the letters) unless scb_set_host_pack turned that off; the lane is then marked
+// prepacked, so its batch skips the device packing.
 scb_status upload_chunk(scb_ctx* ctx, Lane& L, const uint8_t* seqs, const uint64_t* offsets, const Chunk& c) {
     const uint64_t n_seqs = c.seq1 - c.seq0, n_bytes = c.byte1 - c.byte0;
     SCB_TRY(ensure_lane(ctx, L, n_bytes, n_seqs));
     cudaStream_t st = L.stream;
-    if (n_bytes) SCB_CUDA(cudaMemcpyAsync(L.ascii.p, seqs + c.byte0, n_bytes, cudaMemcpyHostToDevice, st));
+    L.prepacked = false;
+    if (ctx->host_pack && n_bytes >= kHostPackMin) {
+        // a graph of this batch sizes the lane's work buffers for its byte class: grow them before
+        // the copy, so that no later growth drops the copied words
+        SCB_TRY(ensure_lane_work(ctx, L, std::max(n_bytes, std::min(class_bytes(n_bytes), kMaxBatchBytes - 64))));
+        SCB_TRY(host_pack_upload(ctx, L, seqs + c.byte0, n_bytes, st));
+        L.prepacked = true;
+    } else if (n_bytes) {
+        SCB_CUDA(cudaMemcpyAsync(L.ascii.p, seqs + c.byte0, n_bytes, cudaMemcpyHostToDevice, st));
+        ctx->h2d_bytes += n_bytes;
+    }
     SCB_CUDA(cudaMemcpyAsync(L.offsets.p, offsets + c.seq0, (n_seqs + 1) * 8, cudaMemcpyHostToDevice, st));
-    ctx->h2d_bytes += n_bytes + (n_seqs + 1) * 8;
+    ctx->h2d_bytes += (n_seqs + 1) * 8;
     if (c.byte0) {
         k_rebase<<<(unsigned)((n_seqs + 1 + 255) / 256), 256, 0, st>>>(L.offsets.as<uint64_t>(), n_seqs + 1, c.byte0);
         note_launch();
@@ -1266,6 +1326,7 @@ scb_status scb_insert_batch_device(scb_ctx* ctx, const uint8_t* d_seqs, const ui
     if (n_bytes > kMaxBatchBytes - 64) return fail_kind(SCB_ERR_INTERNAL_STATE, "device batch above 2 GiB");
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     Lane& L = ctx->lane;
+    L.prepacked = false;  // device input: the batch packs on the device
     unsigned long long c[kCntSlots] = {};
     SCB_TRY(run_batch(ctx, L, kBatchInsert, d_seqs, d_offsets, n, n_bytes, st, c, nullptr));
     ctx->inserted_kmers += c[kCntWindows];
@@ -1309,6 +1370,7 @@ scb_status scb_query_report_device(scb_ctx* ctx, const uint8_t* d_seqs, const ui
     if (n_bytes > kMaxBatchBytes - 64) return fail_kind(SCB_ERR_INTERNAL_STATE, "device batch above 2 GiB");
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     Lane& L = ctx->lane;
+    L.prepacked = false;  // device input: the batch packs on the device
     unsigned long long c[kCntSlots] = {};
     SCB_TRY(run_batch(ctx, L, kBatchReport, d_seqs, d_offsets, n, n_bytes, st, nullptr, c));
     rep->records_processed = c[kCntRecords];
@@ -1364,6 +1426,7 @@ scb_status scb_query_batch_device(scb_ctx* ctx, const uint8_t* d_seqs, const uin
     if (n_bytes > kMaxBatchBytes - 64) return fail_kind(SCB_ERR_INTERNAL_STATE, "device batch above 2 GiB");
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     Lane& L = ctx->lane;
+    L.prepacked = false;  // device input: the batch packs on the device
     SCB_TRY(ensure_lane_work(ctx, L, n_bytes));
     TileArgs a;
     SCB_TRY(prepare_batch(ctx, L, d_seqs, d_offsets, n, n_bytes, st, a));
@@ -1446,29 +1509,6 @@ static scb_status preload_first_piece(scb_ctx* ctx, const uint8_t* seqs, const u
     SCB_CUDA(cudaMemcpyAsync(L.ascii.p, seqs + offsets[0], first, cudaMemcpyHostToDevice, ctx->copy_stream));
     ctx->h2d_bytes += first;
     pre = first;
-    return SCB_OK;
-}
-
-// Pinned staging for host-packed pieces of up to `groups` 32-byte groups: two areas, so the host
-// packs piece p + 1 while piece p's copy reads the other.
-static scb_status ensure_staging(scb_ctx* ctx, uint64_t groups) {
-    for (int i = 0; i < 2; i++) {
-        if (!ctx->stage_free[i]) SCB_CUDA(cudaEventCreateWithFlags(&ctx->stage_free[i], cudaEventDisableTiming));
-    }
-    if (groups <= ctx->stage_groups) return SCB_OK;
-    SCB_CUDA(cudaStreamSynchronize(ctx->copy_stream));
-    for (int i = 0; i < 2; i++) {
-        if (ctx->stage_codes[i]) cudaFreeHost(ctx->stage_codes[i]);
-        if (ctx->stage_valid[i]) cudaFreeHost(ctx->stage_valid[i]);
-        ctx->stage_codes[i] = nullptr;
-        ctx->stage_valid[i] = nullptr;
-    }
-    ctx->stage_groups = 0;
-    for (int i = 0; i < 2; i++) {
-        SCB_CUDA(cudaMallocHost((void**)&ctx->stage_codes[i], (2 * groups + kPadWords) * 4));
-        SCB_CUDA(cudaMallocHost((void**)&ctx->stage_valid[i], (groups + kPadWords) * 4));
-    }
-    ctx->stage_groups = groups;
     return SCB_OK;
 }
 
@@ -1668,6 +1708,7 @@ scb_status scb_build_and_stream_query_device(scb_ctx* ctx, const uint8_t* d_seqs
     if (ctx->frozen) return fail_kind(SCB_ERR_INTERNAL_STATE, "the index is frozen; inserts need a builder");
     if (n_bytes > kMaxBatchBytes - 64) return fail_kind(SCB_ERR_INTERNAL_STATE, "device batch above 2 GiB");
     Lane& L = ctx->lane;
+    L.prepacked = false;  // device input: the batch packs on the device
     return build_stream_batch(ctx, L, d_seqs, d_offsets, n, n_bytes, reinterpret_cast<cudaStream_t>(stream), kmers,
                               smers, rep);
 }
