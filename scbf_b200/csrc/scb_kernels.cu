@@ -486,7 +486,10 @@ __global__ void __launch_bounds__(kTileThreads, 8) k_tiles(TileArgs a) {
     const uint32_t ks = kv - g.s;
     // modes that read a block id for every valid window (the cut computes it at ends only)
     constexpr bool kBlockPerWindow = MODE == kModeInsert || MODE == kModeReport || MODE == kModeAbund ||
-                                     MODE == kModeDistinct || MODE == kModeMaterialize;
+                                     MODE == kModeDistinct || MODE == kModeAbundDistinct ||
+                                     MODE == kModeMaterialize;
+    constexpr bool kAbund = MODE == kModeAbund || MODE == kModeAbundDistinct;
+    constexpr bool kDistinct = MODE == kModeDistinct || MODE == kModeAbundDistinct;
     // batch sizes: from the parameter block on graph replays, else from the arguments
     uint64_t n_bytes = a.n_bytes, n_seqs = a.n_seqs, n_code_words = a.n_code_words, n_bit_words = a.n_bit_words;
     uint32_t n_tiles = a.n_tiles;
@@ -531,7 +534,7 @@ __global__ void __launch_bounds__(kTileThreads, 8) k_tiles(TileArgs a) {
             sm.valid[i] = in ? __ldg(a.valid + bw0 + i) : 0u;
             sm.start[i] = in ? __ldg(a.seqstart + bw0 + i) : 0u;
         }
-        if (MODE == kModeAbund && tid == 0) {
+        if (kAbund && tid == 0) {
             sm.seq_lo = seq_of(offsets, 0, n_seqs, t0);
             const uint64_t last = t0 + kTileWindows;
             sm.seq_hi = seq_of(offsets, sm.seq_lo, n_seqs, last);
@@ -632,7 +635,7 @@ __global__ void __launch_bounds__(kTileThreads, 8) k_tiles(TileArgs a) {
                 insert_smer<BITS>(table32, g, block_base(g, sm.block[e]), smer, a.status);
                 c_smer++;
             }
-        } else if constexpr (MODE == kModeReport || MODE == kModeAbund || MODE == kModeDistinct) {
+        } else if constexpr (MODE == kModeReport || kAbund || kDistinct) {
             for (uint32_t i = tid; i < kTileWindows; i += blockDim.x) {
                 if (sm.poff[i] == kNoWindow) continue;
                 const uint64_t pos = t0 + i;
@@ -641,12 +644,14 @@ __global__ void __launch_bounds__(kTileThreads, 8) k_tiles(TileArgs a) {
                     c_valid++;
                     c_pos += r > 0;
                     c_sum += r;
-                } else if constexpr (MODE == kModeAbund) {
+                }
+                if constexpr (kAbund) {
                     const uint64_t j = seq_of(offsets, sm.seq_lo, sm.seq_hi, pos);
                     const uint64_t o = a.woff[j] + (pos - __ldg(offsets + j));
                     a.out[o] = r;
                     a.out_valid[o] = 1;
-                } else {
+                }
+                if constexpr (kDistinct) {
                     c_valid++;
                     const uint64_t key = canonical(codes64(sm.codes, pos - cb) & len_mask(kv), kv);
                     if (set_insert(a.set_keys, a.set_mask, key, a.status)) {
@@ -844,6 +849,7 @@ void launch_tiles(int mode, const TileArgs& a, int grid, cudaStream_t st) {
         case kModeReport: launch_tiles_bits<kModeReport>(a, grid, st); break;
         case kModeAbund: launch_tiles_bits<kModeAbund>(a, grid, st); break;
         case kModeDistinct: launch_tiles_bits<kModeDistinct>(a, grid, st); break;
+        case kModeAbundDistinct: launch_tiles_bits<kModeAbundDistinct>(a, grid, st); break;
         case kModeStats: launch_tiles_bits<kModeStats>(a, grid, st); break;
         case kModeDebugMin: launch_tiles_bits<kModeDebugMin>(a, grid, st); break;
         case kModeMaterialize: launch_tiles_bits<kModeMaterialize>(a, grid, st); break;
@@ -863,6 +869,7 @@ int tile_grid(int mode, int bits, int sm_count, uint32_t n_tiles) {
         case kModeReport: SCB_PICK(kModeReport); break;
         case kModeAbund: SCB_PICK(kModeAbund); break;
         case kModeDistinct: SCB_PICK(kModeDistinct); break;
+        case kModeAbundDistinct: SCB_PICK(kModeAbundDistinct); break;
         case kModeStats: SCB_PICK(kModeStats); break;
         case kModeDebugMin: SCB_PICK(kModeDebugMin); break;
         case kModeCut: SCB_PICK(kModeCut); break;

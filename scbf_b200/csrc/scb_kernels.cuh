@@ -28,8 +28,10 @@ enum TileMode : int {
     kModeCut = 8,          // (b) for the grouped pipeline: one record per super-k-mer + bucket counts
     kModeBuild = 9,        // grouped apply of a build + stream query: insert a bucket's records, commit,
                            // then answer the same records' query from the committed shared-memory block
-    kModeSpectrum = 10     // grouped distinct-k-mer spectrum: a bucket's windows' estimates from its staged
+    kModeSpectrum = 10,    // grouped distinct-k-mer spectrum: a bucket's windows' estimates from its staged
                            // blocks, their canonical k-mers deduplicated in shared memory
+    kModeAbundDistinct = 11  // kModeAbund and kModeDistinct from one estimate per window (a serving batch
+                             // that also feeds the whole-stream spectrum)
 };
 
 // Sizes and input pointers of one batch, in device memory: a graph captured for a shape class

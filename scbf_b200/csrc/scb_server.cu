@@ -6,7 +6,8 @@
 // all slots together fit the configured device-memory budget (admission control).  Whenever a
 // slot is free and pieces are pending, the scheduler packs the oldest pieces into a batch and
 // launches it on the slot's stream: H2D copy, 2-bit packing, the fused per-window abundance
-// kernel, D2H copy.  The device work of a batch (clears, packing, sequence starts, abundance
+// kernel (which, with the whole-stream spectrum on, also feeds the stream's distinct-k-mer set
+// from the same estimates), D2H copy.  The device work of a batch (clears, packing, sequence starts, abundance
 // kernel) is one replay of a CUDA graph captured once per slot: the batch's sizes reach the
 // kernels through a parameter block that a one-thread kernel writes before the replay, and the
 // kernels' grids do not depend on the batch, so the same graph serves every batch shape.
@@ -15,7 +16,8 @@
 // wakes the scheduler, which scatters the results into the requests' output buffers and
 // completes the requests whose pieces are all done.  Each slot has its own completion thread,
 // which copies its batch's results out of pinned memory into the requests' buffers outside the
-// server lock, so the copies of different slots run in parallel and never hold up the scheduler.
+// server lock (a large batch with helper threads), so the copies of different slots run in
+// parallel and never hold up the scheduler.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -125,6 +127,8 @@ struct scb_server {
 
     void run();
     void finish(Slot& s);
+    void copy_out(Slot& s);
+    uint64_t host_share = 1;  // threads a slot's copy-out may use: the host's threads / slots
     std::atomic<bool> stop_finishers{false};
     void add_spectrum(TileArgs& d, unsigned int* tile_counter) const;
     scb_status clear_spectrum(cudaStream_t st);
@@ -175,8 +179,9 @@ static TileArgs tile_args(const scb_server& srv, const Slot& s, uint64_t bytes, 
     return a;
 }
 
-// Distinct-k-mer pass of a batch into the server's stream-wide set (kernel (f), kModeDistinct):
-// the same windows and estimates as the abundance pass, each new canonical k-mer counted once.
+// Points a batch's tile arguments at the server's stream-wide distinct-k-mer set (kernel (f)): the
+// abundance kernel in its kModeAbundDistinct form also inserts each window's canonical k-mer and
+// counts the estimate of every new one.
 void scb_server::add_spectrum(TileArgs& d, unsigned int* tile_counter) const {
     d.cnt = spec_cnt.as<unsigned long long>();
     d.tile_counter = tile_counter;
@@ -208,11 +213,11 @@ scb_status scb_server::record(Slot& s, cudaStream_t st) {
     // capacities of the slot; the tile kernel reads the batch's sizes from bp
     TileArgs a = tile_args(*this, s, cfg.max_batch_bytes, cfg.max_batch_seqs);
     a.dyn = bp;
-    launch_tiles(kModeAbund, a, tile_grid(kModeAbund, ctx->g.bits, sms, a.n_tiles), st);
-    if (spectrum) {
-        TileArgs d = a;
-        add_spectrum(d, s.tiles.as<unsigned int>() + 1);
-        launch_tiles(kModeDistinct, d, tile_grid(kModeDistinct, ctx->g.bits, sms, d.n_tiles), st);
+    if (spectrum) {  // one estimate per window serves the abundances and the stream's key set
+        add_spectrum(a, s.tiles.as<unsigned int>());
+        launch_tiles(kModeAbundDistinct, a, tile_grid(kModeAbundDistinct, ctx->g.bits, sms, a.n_tiles), st);
+    } else {
+        launch_tiles(kModeAbund, a, tile_grid(kModeAbund, ctx->g.bits, sms, a.n_tiles), st);
     }
     SCB_CUDA(cudaGetLastError());
     return SCB_OK;
@@ -285,11 +290,12 @@ scb_status scb_server::launch(Slot& s) {
             launch_pack(s.ascii.as<uint8_t>(), bytes, s.codes.as<uint32_t>(), s.valid.as<uint32_t>(), st);
             launch_seqstart(s.offsets.as<uint64_t>(), seqs, bytes, s.seqstart.as<uint32_t>(), st);
             TileArgs a = tile_args(*this, s, bytes, seqs);
-            launch_tiles(kModeAbund, a, tile_grid(kModeAbund, c->g.bits, c->sm_count, a.n_tiles), st);
             if (spectrum) {
-                TileArgs d = a;
-                add_spectrum(d, s.tiles.as<unsigned int>() + 1);
-                launch_tiles(kModeDistinct, d, tile_grid(kModeDistinct, c->g.bits, c->sm_count, d.n_tiles), st);
+                add_spectrum(a, s.tiles.as<unsigned int>());
+                launch_tiles(kModeAbundDistinct, a, tile_grid(kModeAbundDistinct, c->g.bits, c->sm_count, a.n_tiles),
+                             st);
+            } else {
+                launch_tiles(kModeAbund, a, tile_grid(kModeAbund, c->g.bits, c->sm_count, a.n_tiles), st);
             }
             SCB_CUDA(cudaGetLastError());
         }
@@ -311,6 +317,50 @@ scb_status scb_server::launch(Slot& s) {
     return SCB_OK;
 }
 
+// Copies a finished batch's per-window results from the slot's pinned buffers into the requests'
+// buffers.  A large batch (9 bytes per window: a full 16 MiB batch is about 150 MB) is split into
+// pieces of at least 4 MiB that host_share threads copy together (the host's threads divided
+// among the slots), so the copy-out keeps up with the GPU instead of holding the slot.
+void scb_server::copy_out(Slot& s) {
+    struct Part {
+        uint8_t* dst;
+        const uint8_t* src;
+        uint64_t bytes;
+    };
+    constexpr uint64_t kPart = 4ull << 20;
+    std::vector<Part> parts;
+    uint64_t total = 0;
+    auto add = [&](uint8_t* dst, const uint8_t* src, uint64_t bytes) {
+        for (uint64_t off = 0; off < bytes; off += kPart) {
+            parts.push_back(Part{dst + off, src + off, std::min(kPart, bytes - off)});
+        }
+        total += bytes;
+    };
+    for (size_t i = 0; i < s.pieces.size(); i++) {
+        const Piece& p = s.pieces[i];
+        if (!p.windows) continue;
+        add(reinterpret_cast<uint8_t*>(p.req->out + p.win0), reinterpret_cast<const uint8_t*>(s.h_out + s.piece_win[i]),
+            p.windows * 8);
+        add(p.req->valid + p.win0, s.h_outv + s.piece_win[i], p.windows);
+    }
+    const unsigned helpers = (unsigned)std::min<uint64_t>(host_share, parts.size()) - 1u;
+    if (helpers == 0 || total < 2 * kPart) {
+        for (const Part& q : parts) std::memcpy(q.dst, q.src, q.bytes);
+        return;
+    }
+    std::atomic<size_t> next{0};
+    auto work = [&] {
+        for (size_t i = next.fetch_add(1); i < parts.size(); i = next.fetch_add(1)) {
+            std::memcpy(parts[i].dst, parts[i].src, parts[i].bytes);
+        }
+    };
+    std::vector<std::thread> th;
+    th.reserve(helpers);
+    for (unsigned t = 0; t < helpers; t++) th.emplace_back(work);
+    work();
+    for (auto& x : th) x.join();
+}
+
 // The slot's completion thread: waits for its batch's host callback (polling every 100 us, so a
 // notification that arrives before the wait is never lost for long), copies the results into the
 // requests' buffers without the server lock (a request's buffers stay valid until its wait returns,
@@ -327,13 +377,7 @@ void scb_server::finish(Slot& s) {
             if (stop_finishers.load()) break;
             continue;
         }
-        for (size_t i = 0; i < s.pieces.size(); i++) {
-            const Piece& p = s.pieces[i];
-            if (p.windows) {
-                std::memcpy(p.req->out + p.win0, s.h_out + s.piece_win[i], p.windows * 8);
-                std::memcpy(p.req->valid + p.win0, s.h_outv + s.piece_win[i], p.windows);
-            }
-        }
+        copy_out(s);
         std::lock_guard<std::mutex> lk(mu);
         s.complete.store(false, std::memory_order_relaxed);
         complete(s);
@@ -436,6 +480,7 @@ scb_status scb_server_create(scb_ctx* ctx, const scb_server_config* cfg_in, scb_
     srv->ctx = ctx;
     srv->cfg = cfg;
     srv->cfg.max_inflight = (uint32_t)n_slots;
+    srv->host_share = std::max<uint64_t>(1, std::thread::hardware_concurrency() / n_slots);
     srv->use_graphs = ctx->graphs;
     for (uint64_t i = 0; i < n_slots; i++) {
         auto s = std::make_unique<Slot>();

@@ -101,14 +101,15 @@ def test_memory_budget_admits_one_small_batch_at_a_time(index_and_requests):
 def test_whole_stream_spectrum_equals_batch_spectrum(index_and_requests, oracle_mod):
     """A server with spectrum_keys adds every answered window's canonical k-mer to one device set;
     at the end of the stream its spectrum equals the distinct-k-mer spectrum of all the requests'
-    sequences at once (src/fastx.rs:255-308, 392-410), which the oracle checks too."""
+    sequences at once (src/fastx.rs:255-308, 392-410), which the oracle checks too, and every
+    request's abundances equal the per-call query's."""
     import scbf_b200 as scb
 
     idx, requests, expected = index_and_requests
     srv = scb.SuperCountingBloomServer(idx, max_batch_bytes=2 << 20, max_inflight=4, spectrum_keys=4_000_000)
     tickets = [srv.submit(d, o) for d, o in requests + requests[:5]]  # repeats add no distinct k-mer
-    for t in tickets:
-        srv.wait(t)
+    # the same kernel answers the windows and feeds the set: the abundances stay the per-call query's
+    _check_all([srv.wait(t)[:2] for t in tickets], expected + expected[:5])
     got = srv.spectrum()
     seqs = [bytes(d[int(o[i]):int(o[i + 1])]) for d, o in requests for i in range(len(o) - 1)]
     data, offsets = scb.pack_sequences(seqs)
