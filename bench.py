@@ -561,6 +561,7 @@ def run_ours(args, dist: Dist):
         check(L.scb_freeze(c1.h))
         spectrum["config1"] = run_spectrum(L, c1.h, d1, o1, st1, 24)
         c1.close()
+    config1 = run_config1(L, args)
     serving = None
     if not args.no_serve:
         check(L.scb_set_strategy(h, 0, 0))
@@ -592,7 +593,8 @@ def run_ours(args, dist: Dist):
             "stage_ms": {k_: info[k_] for k_ in ("pack_ms", "insert_ms", "query_ms", "cut_ms", "bucket_ms",
                                                  "apply_insert_ms", "apply_query_ms")},
             "tuning": tuning, "graphs": graphs,
-            "plain": plain, "strategies": strategies, "mixed": mixed, "serve": serving, "e2e": e2e,
+            "plain": plain, "strategies": strategies, "mixed": mixed, "serve": serving, "config1": config1,
+            "e2e": e2e,
             "spectrum": spectrum,
             "roofline": roofline,
             "cpu_baseline": cpu,
@@ -656,6 +658,57 @@ def run_spectrum(L, h, data, offsets, st, slot_exp: int, reps: int = 2) -> dict:
                                       "bases + each touched block read once; keys and histogram stay in shared "
                                       "memory"}})
     return out
+
+
+def run_config1(L, args) -> dict:
+    """Configuration 1 (1 Mbp genome, 30x of 150 bp reads, 2^24 16-bit slots: the 32 MiB table fits
+    in L2), the same build + stream query step on reads resident in HBM, CUDA events on the stream.
+    With the counters in L2 the rate is also given as counter updates per second (s-mers x
+    n_hashes), the L2-atomic figure the configuration asks for."""
+    import torch
+
+    from scbf_b200 import _lib, api
+    from scbf_b200 import workloads as wl
+
+    d1, o1 = wl.config1()
+    cfg1 = api.SuperCountingBloomConfig(k=GEOM["k"], m=GEOM["m"], s=GEOM["s"], n_hashes=GEOM["n_hashes"],
+                                        counter_bits=api.CounterBits(16), counter_slots_exponent=24,
+                                        block_slots_exponent=GEOM["block_slots_exponent"], threads=1, queue=4096)
+    c1 = api._create(cfg1)
+    dd = torch.from_numpy(d1).cuda()
+    do = torch.from_numpy(o1.view(np.int64)).cuda()
+    n, nb = len(o1) - 1, int(o1[-1])
+    stream = torch.cuda.current_stream()
+    sp = C.c_void_p(stream.cuda_stream)
+    km, sm = C.c_uint64(0), C.c_uint64(0)
+    rep = _lib.ScbReport()
+
+    def check(st):
+        if st != 0:
+            raise RuntimeError(_lib.last_error())
+
+    def step():
+        check(L.scb_reset(c1.h))
+        check(L.scb_build_and_stream_query_device(c1.h, dd.data_ptr(), do.data_ptr(), n, nb, sp, C.byref(km),
+                                                  C.byref(sm), C.byref(rep)))
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    steps = 20
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(steps):
+        step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / steps
+    c1.close()
+    return {"workload": "configuration 1: 1 Mbp uniform genome, 30x of 150 bp reads (200 000 reads), 0.5% "
+                        "substitutions; 2^24 16-bit slots (32 MiB, resident in L2)",
+            "kmers": km.value, "smers": sm.value, "ms_per_step": ms, "kmers_per_s": km.value / (ms / 1e3),
+            "counter_updates_per_s": sm.value * GEOM["n_hashes"] / (ms / 1e3),
+            "note": "build + stream query per step, reads resident in HBM; the step includes the table clear"}
 
 
 def run_serving(ctx, args, rank: int) -> dict:

@@ -577,12 +577,23 @@ __global__ void __launch_bounds__(kTileThreads, 8) k_tiles(TileArgs a) {
             const uint64_t vb = bits64(sm.valid, pos0 - bb), sb = bits64(sm.start, pos0 - bb);
             uint32_t lm[4], rm[4];
             strip_minima(sm.pk, i0, wv, lm, rm);
-            uint32_t tg = __popcll(codes64(sm.codes, pos0 - cb) & len_mask(kv) & 0xAAAAAAAAAAAAAAAAull);
+            // the T/G count of each window (bit 1 of a base's code), rolled one base at a time; with
+            // k compiled in, the bases that leave and enter come from two 64-bit reads of the codes
+            const uint64_t c_lo = codes64(sm.codes, pos0 - cb);  // bases pos0 .. pos0 + 31
+            const uint64_t c_hi = KMC ? codes64(sm.codes, pos0 - cb + 32) : 0ull;
+            uint32_t tg = __popcll(c_lo & len_mask(kv) & 0xAAAAAAAAAAAAAAAAull);
 #pragma unroll
             for (uint32_t j = 0; j < 4; j++) {
                 if (j > 0) {  // roll the T/G count by one base
-                    const uint64_t out_b = pos0 + j - 1 - cb;
-                    tg += (code_at(sm.codes, out_b + kv) >> 1) - (code_at(sm.codes, out_b) >> 1);
+                    if constexpr (KMC != 0) {
+                        const uint32_t in = j - 1 + kv;  // base entering, relative to pos0
+                        const uint32_t bit_in = in < 32 ? (uint32_t)(c_lo >> (2 * in + 1)) & 1u
+                                                        : (uint32_t)(c_hi >> (2 * (in - 32) + 1)) & 1u;
+                        tg += bit_in - ((uint32_t)(c_lo >> (2 * (j - 1) + 1)) & 1u);
+                    } else {
+                        const uint64_t out_b = pos0 + j - 1 - cb;
+                        tg += (code_at(sm.codes, out_b + kv) >> 1) - (code_at(sm.codes, out_b) >> 1);
+                    }
                 }
                 uint16_t po = kNoWindow;
                 if (window_ok(vb >> j, sb >> j, kv)) {
@@ -750,13 +761,24 @@ __global__ void __launch_bounds__(kTileThreads, 8) k_tiles(TileArgs a) {
                 sm.warp_run[wid] = rmax;
             }
             __syncthreads();
-            uint32_t before = incl - mine, tile_total = 0;
-            for (uint32_t x = 0; x < kTileThreads / 32; x++) {
-                const uint32_t c = sm.warp_cnt[x];
-                before += x < wid ? c : 0u;
-                tile_total += c;
-                if (x < wid) rprev = max(rprev, sm.warp_run[x]);
+            // the warps' totals: an 8-lane scan of their counts (sum) and run starts (maximum)
+            constexpr uint32_t kWarps = kTileThreads / 32;
+            uint32_t wc = lane < kWarps ? sm.warp_cnt[lane] : 0u;
+            uint32_t wr = lane < kWarps ? sm.warp_run[lane] : 0u;
+#pragma unroll
+            for (uint32_t off = 1; off < kWarps; off <<= 1) {
+                const uint32_t yc = __shfl_up_sync(0xFFFFFFFFu, wc, off);
+                const uint32_t yr = __shfl_up_sync(0xFFFFFFFFu, wr, off);
+                if (lane >= off) {
+                    wc += yc;
+                    wr = max(wr, yr);
+                }
             }
+            const uint32_t tile_total = __shfl_sync(0xFFFFFFFFu, wc, kWarps - 1);
+            const uint32_t prev_c = __shfl_sync(0xFFFFFFFFu, wc, wid ? wid - 1 : 0);
+            const uint32_t prev_r = __shfl_sync(0xFFFFFFFFu, wr, wid ? wid - 1 : 0);
+            uint32_t before = incl - mine + (wid ? prev_c : 0u);
+            if (wid) rprev = max(rprev, prev_r);
             // compact the tile's ends (window | first window << 16, in window order, in the block
             // array the cut does not otherwise use) so the per-record work below runs on full warps
 #pragma unroll
