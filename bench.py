@@ -845,7 +845,7 @@ def run_serving(ctx, args, rank: int) -> dict:
 
     out = {"index": "config-2 frozen index, resident",
            "arrivals": "Poisson; requests drawn from a pool of generated templates (results of one template "
-                       "share an output buffer)"}
+                       "share an output buffer, checked against a direct query after the sweep)"}
     # 1 M-k-mer requests: batched server (with the whole-stream spectrum) vs unbatched
     fixed = pool_fixed(16)
     srv, outs = server(fixed, 16 << 20, spectrum_keys=64 << 20)
@@ -855,6 +855,14 @@ def run_serving(ctx, args, rank: int) -> dict:
         sweep.append(r)
         if knee(r):
             break
+    # every template's output buffer holds the answer of its last request: it must equal one direct
+    # per-window query of the same sequences
+    for (d, o), (ob, vb, nw) in zip(fixed, outs):
+        eo, ev = np.zeros(max(nw, 1), np.uint64), np.zeros(max(nw, 1), np.uint8)
+        if L.scb_query_batch(ctx.h, d.ctypes.data, o.ctypes.data, len(o) - 1, eo.ctypes.data, ev.ctypes.data) != 0:
+            raise RuntimeError(_lib.last_error())
+        assert np.array_equal(vb[:nw], ev[:nw]) and np.array_equal(np.where(ev[:nw] == 1, ob[:nw], 0),
+                                                                   np.where(ev[:nw] == 1, eo[:nw], 0)), "served results"
     t_sp = time.perf_counter()
     rows, dk, qk = C.c_uint64(0), C.c_uint64(0), C.c_uint64(0)
     if L.scb_server_spectrum(srv, None, None, 0, C.byref(rows), C.byref(dk), C.byref(qk)) != 0:
