@@ -736,9 +736,11 @@ def run_serving(ctx, args, rank: int) -> dict:
         return [workloads.random_sequences(40, 25_000, 25_001, seed=1000 + i, genome=genome) for i in range(count)]
 
     def pool_mixed(count):
+        # its own generator: the pool does not depend on how many rates the sweeps before it ran
+        prng = np.random.default_rng(19)
         reqs = []
         for i in range(count):
-            n = int(np.exp(rng.uniform(0, np.log(1e5))))
+            n = int(np.exp(prng.uniform(0, np.log(1e5))))
             reqs.append(workloads.random_sequences(n, 100, 50_000, seed=2000 + i, genome=genome))
         return reqs
 
