@@ -720,7 +720,7 @@ def run_serving(ctx, args, rank: int) -> dict:
       100 ms), through the continuous-batching server;
     - the same requests and rates through the unbatched path: one scb_query_batch per request,
       in arrival order, no overlap (the plain per-request GPU path);
-    - mixed requests, 1-10^5 sequences of log-uniform 100 bp-50 kbp (about 70 Mbp and 630 MB of
+    - mixed requests, 1-10^5 sequences of log-uniform 100 bp-50 kbp (about 90 Mbp and 820 MB of
       per-window output on average, uncapped), at rates up to their knee;
     - the whole-stream distinct-k-mer spectrum, read from the server's set at the end of the 1 M
       stream and checked against the spectrum of the same sequences in one batch."""
