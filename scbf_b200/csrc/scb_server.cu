@@ -7,8 +7,9 @@
 // slot is free and pieces are pending, the scheduler packs the oldest pieces into a batch and
 // launches it on the slot's stream: H2D copy, 2-bit packing, the fused per-window abundance
 // kernel (which, with the whole-stream spectrum on, also feeds the stream's distinct-k-mer set
-// from the same estimates), D2H copy.  The device work of a batch (clears, packing, sequence starts, abundance
-// kernel) is one replay of a CUDA graph captured once per slot: the batch's sizes reach the
+// from the same estimates), narrowing of the estimates to the counters' width, D2H copy.  The
+// device work of a batch (clears, packing, sequence starts, abundance kernel, narrowing) is one
+// replay of a CUDA graph captured once per slot: the batch's sizes reach the
 // kernels through a parameter block that a one-thread kernel writes before the replay, and the
 // kernels' grids do not depend on the batch, so the same graph serves every batch shape.
 // Batches of different slots overlap on the GPU; requests that arrive while
@@ -67,12 +68,13 @@ struct Piece {
 struct Slot {
     cudaStream_t stream = nullptr;
     DevBuf ascii, offsets, woff, codes, valid, seqstart, out, outv, cnt, tiles, params;
+    DevBuf outn;  // the estimates narrowed to the counters' width for the copy to the host
     cudaGraphExec_t graph = nullptr;  // the slot's batch, captured when the server starts
     uint64_t graph_launches = 0;
     uint8_t* h_ascii = nullptr;
     uint64_t* h_offsets = nullptr;
     uint64_t* h_woff = nullptr;
-    uint64_t* h_out = nullptr;
+    uint8_t* h_outn = nullptr;  // narrowed estimates (2 or 4 bytes per window)
     uint8_t* h_outv = nullptr;
     std::vector<Piece> pieces;
     std::vector<uint64_t> piece_win;  // first window of each piece inside the batch output
@@ -87,7 +89,7 @@ struct Slot {
         if (h_ascii) cudaFreeHost(h_ascii);
         if (h_offsets) cudaFreeHost(h_offsets);
         if (h_woff) cudaFreeHost(h_woff);
-        if (h_out) cudaFreeHost(h_out);
+        if (h_outn) cudaFreeHost(h_outn);
         if (h_outv) cudaFreeHost(h_outv);
         if (stream) cudaStreamDestroy(stream);
     }
@@ -115,6 +117,9 @@ struct scb_server {
     uint64_t stat_windows = 0, stat_batches = 0;
     bool use_graphs = true;
     uint64_t captures = 0, replays = 0;
+    // bytes per window of the estimates copied to the host: 2 for 8- and 16-bit counters, 4 for
+    // 32-bit ones (an estimate never exceeds the counters' maximum); widened to u64 on the host
+    uint32_t out_width = 2;
     // whole-stream spectrum: distinct canonical k-mers of every batch (set of 2^k keys, ~0 empty),
     // the dense histogram of their estimates, values past it (32-bit counters), and the counters
     // the distinct kernel adds to (windows, distinct keys, overflow entries)
@@ -201,6 +206,23 @@ scb_status scb_server::clear_spectrum(cudaStream_t st) {
     return SCB_OK;
 }
 
+// Narrows a batch's u64 estimates (out, cleared past the batch's windows) to `width` bytes each
+// for the copy to the host: the first n entries, or the batch's byte count (an upper bound of its
+// windows) from the parameter block on graph replays.
+__global__ void k_narrow_out(const BatchParams* __restrict__ bp, uint64_t n, const unsigned long long* __restrict__ out,
+                             void* __restrict__ outn, uint32_t width) {
+    if (bp) n = bp->n_bytes;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const unsigned long long v = __ldcs(out + i);
+        if (width == 2) {
+            static_cast<uint16_t*>(outn)[i] = (uint16_t)v;
+        } else {
+            static_cast<uint32_t*>(outn)[i] = (uint32_t)v;
+        }
+    }
+}
+
 // The graph body of one slot batch: sizes from the slot's parameter block, fixed grids.
 scb_status scb_server::record(Slot& s, cudaStream_t st) {
     const BatchParams* bp = s.params.as<BatchParams>();
@@ -219,6 +241,8 @@ scb_status scb_server::record(Slot& s, cudaStream_t st) {
     } else {
         launch_tiles(kModeAbund, a, tile_grid(kModeAbund, ctx->g.bits, sms, a.n_tiles), st);
     }
+    k_narrow_out<<<(unsigned)(sms * 4), 256, 0, st>>>(bp, 0, s.out.as<unsigned long long>(), s.outn.p, out_width);
+    note_launch();
     SCB_CUDA(cudaGetLastError());
     return SCB_OK;
 }
@@ -297,11 +321,16 @@ scb_status scb_server::launch(Slot& s) {
             } else {
                 launch_tiles(kModeAbund, a, tile_grid(kModeAbund, c->g.bits, c->sm_count, a.n_tiles), st);
             }
+            if (wins) {
+                k_narrow_out<<<(unsigned)(c->sm_count * 4), 256, 0, st>>>(nullptr, wins, s.out.as<unsigned long long>(),
+                                                                           s.outn.p, out_width);
+                note_launch();
+            }
             SCB_CUDA(cudaGetLastError());
         }
     }
     if (wins) {
-        SCB_CUDA(cudaMemcpyAsync(s.h_out, s.out.p, wins * 8, cudaMemcpyDeviceToHost, st));
+        SCB_CUDA(cudaMemcpyAsync(s.h_outn, s.outn.p, wins * out_width, cudaMemcpyDeviceToHost, st));
         SCB_CUDA(cudaMemcpyAsync(s.h_outv, s.outv.p, wins, cudaMemcpyDeviceToHost, st));
     }
     s.complete.store(false, std::memory_order_relaxed);
@@ -318,41 +347,49 @@ scb_status scb_server::launch(Slot& s) {
 }
 
 // Copies a finished batch's per-window results from the slot's pinned buffers into the requests'
-// buffers.  A large batch (9 bytes per window: a full 16 MiB batch is about 150 MB) is split into
-// pieces of at least 4 MiB that host_share threads copy together (the host's threads divided
-// among the slots), so the copy-out keeps up with the GPU instead of holding the slot.
+// buffers, widening the estimates to u64 (the validity bytes are copied as they are).  A large
+// batch (a full 16 MiB batch writes about 150 MB into the requests) is split into parts of 512 Ki
+// windows that host_share threads work through together (the host's threads divided among the
+// slots), so the copy-out keeps up with the GPU instead of holding the slot.
 void scb_server::copy_out(Slot& s) {
     struct Part {
-        uint8_t* dst;
-        const uint8_t* src;
-        uint64_t bytes;
+        uint64_t* est;           // the request's estimates
+        uint8_t* valid;          // and validity bytes
+        const uint8_t* src;      // the slot's narrowed estimates of the first window
+        const uint8_t* src_valid;
+        uint64_t n;              // windows
     };
-    constexpr uint64_t kPart = 4ull << 20;
+    constexpr uint64_t kPart = 512ull << 10;
+    const uint32_t w = out_width;
     std::vector<Part> parts;
     uint64_t total = 0;
-    auto add = [&](uint8_t* dst, const uint8_t* src, uint64_t bytes) {
-        for (uint64_t off = 0; off < bytes; off += kPart) {
-            parts.push_back(Part{dst + off, src + off, std::min(kPart, bytes - off)});
-        }
-        total += bytes;
-    };
     for (size_t i = 0; i < s.pieces.size(); i++) {
         const Piece& p = s.pieces[i];
-        if (!p.windows) continue;
-        add(reinterpret_cast<uint8_t*>(p.req->out + p.win0), reinterpret_cast<const uint8_t*>(s.h_out + s.piece_win[i]),
-            p.windows * 8);
-        add(p.req->valid + p.win0, s.h_outv + s.piece_win[i], p.windows);
+        for (uint64_t off = 0; off < p.windows; off += kPart) {
+            const uint64_t b = s.piece_win[i] + off;
+            parts.push_back(Part{p.req->out + p.win0 + off, p.req->valid + p.win0 + off, s.h_outn + b * w,
+                                 s.h_outv + b, std::min(kPart, p.windows - off)});
+        }
+        total += p.windows;
     }
+    auto run = [w](const Part& q) {
+        if (w == 2) {
+            const uint16_t* src = reinterpret_cast<const uint16_t*>(q.src);
+            for (uint64_t j = 0; j < q.n; j++) q.est[j] = src[j];
+        } else {
+            const uint32_t* src = reinterpret_cast<const uint32_t*>(q.src);
+            for (uint64_t j = 0; j < q.n; j++) q.est[j] = src[j];
+        }
+        std::memcpy(q.valid, q.src_valid, q.n);
+    };
     const unsigned helpers = (unsigned)std::min<uint64_t>(host_share, parts.size()) - 1u;
     if (helpers == 0 || total < 2 * kPart) {
-        for (const Part& q : parts) std::memcpy(q.dst, q.src, q.bytes);
+        for (const Part& q : parts) run(q);
         return;
     }
     std::atomic<size_t> next{0};
     auto work = [&] {
-        for (size_t i = next.fetch_add(1); i < parts.size(); i = next.fetch_add(1)) {
-            std::memcpy(parts[i].dst, parts[i].src, parts[i].bytes);
-        }
+        for (size_t i = next.fetch_add(1); i < parts.size(); i = next.fetch_add(1)) run(parts[i]);
     };
     std::vector<std::thread> th;
     th.reserve(helpers);
@@ -465,11 +502,11 @@ scb_status scb_server_create(scb_ctx* ctx, const scb_server_config* cfg_in, scb_
     if (cfg.max_batch_bytes > kMaxBatchBytes / 2)
         return fail_kind(SCB_ERR_INVALID_CONFIG, "max_batch_bytes above 1 GiB");
     // device bytes of one slot: reads, 2-bit codes, two bitmaps, offsets, window offsets,
-    // u64 + u8 outputs per window (at most one window per byte)
+    // u64 + u8 outputs and the narrowed u16/u32 copy per window (at most one window per byte)
     const uint64_t B = cfg.max_batch_bytes, R = cfg.max_batch_seqs;
     const uint64_t groups = (B + 31) / 32;
     const uint64_t slot_bytes = (groups * 32 + 64) + (2 * groups + kPadWords) * 4 + 2 * (groups + kPadWords) * 4 +
-                                (R + 1) * 8 * 2 + B * 9 + kCntSlots * 8 + 64;
+                                (R + 1) * 8 * 2 + B * 13 + kCntSlots * 8 + 64;
     uint64_t n_slots = cfg.memory_budget_bytes ? cfg.memory_budget_bytes / slot_bytes : cfg.max_inflight;
     n_slots = std::min<uint64_t>(n_slots, cfg.max_inflight);
     if (n_slots == 0)
@@ -482,6 +519,7 @@ scb_status scb_server_create(scb_ctx* ctx, const scb_server_config* cfg_in, scb_
     srv->cfg.max_inflight = (uint32_t)n_slots;
     srv->host_share = std::max<uint64_t>(1, std::thread::hardware_concurrency() / n_slots);
     srv->use_graphs = ctx->graphs;
+    srv->out_width = ctx->g.bits <= 16 ? 2u : 4u;
     for (uint64_t i = 0; i < n_slots; i++) {
         auto s = std::make_unique<Slot>();
         SCB_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
@@ -492,6 +530,7 @@ scb_status scb_server_create(scb_ctx* ctx, const scb_server_config* cfg_in, scb_
         SCB_TRY(s->valid.ensure((groups + kPadWords) * 4));
         SCB_TRY(s->seqstart.ensure((groups + kPadWords) * 4));
         SCB_TRY(s->out.ensure(std::max<uint64_t>(B, 1) * 8));
+        SCB_TRY(s->outn.ensure(std::max<uint64_t>(B, 1) * 4));
         SCB_TRY(s->outv.ensure(B + 16));  // cleared in 16-byte stores
         SCB_TRY(s->cnt.ensure(kCntSlots * 8));
         SCB_TRY(s->tiles.ensure(64));
@@ -499,7 +538,7 @@ scb_status scb_server_create(scb_ctx* ctx, const scb_server_config* cfg_in, scb_
         SCB_CUDA(cudaMallocHost((void**)&s->h_ascii, B + 64));
         SCB_CUDA(cudaMallocHost((void**)&s->h_offsets, (R + 1) * 8));
         SCB_CUDA(cudaMallocHost((void**)&s->h_woff, (R + 1) * 8));
-        SCB_CUDA(cudaMallocHost((void**)&s->h_out, std::max<uint64_t>(B, 1) * 8));
+        SCB_CUDA(cudaMallocHost((void**)&s->h_outn, std::max<uint64_t>(B, 1) * srv->out_width));
         SCB_CUDA(cudaMallocHost((void**)&s->h_outv, std::max<uint64_t>(B, 1)));
         srv->slots.push_back(std::move(s));
     }

@@ -130,3 +130,29 @@ def test_whole_stream_spectrum_equals_batch_spectrum(index_and_requests, oracle_
     empty = srv.spectrum()
     assert empty["rows"] == [] and empty["distinct_keys"] == 0
     srv.close()
+
+
+@pytest.mark.parametrize("bits", [8, 32])
+def test_served_estimates_cross_at_the_counters_width(bits):
+    """The server copies each window's estimate to the host at the counters' width (2 bytes for 8-
+    and 16-bit counters, 4 for 32-bit ones) and widens it to u64 there: results equal the per-call
+    query for 8-bit counters (saturated at 255) and 32-bit ones, in batches large enough that the
+    copy-out is split over several threads."""
+    import scbf_b200 as scb
+    from scbf_b200 import workloads
+
+    genome = workloads.random_genome(200_000, seed=41)
+    data, offsets = workloads.short_reads(n_reads=40_000, read_len=150, seed=42, sub_rate=0.01, genome=genome)
+    cfg = scb.SuperCountingBloomConfig(counter_slots_exponent=18, counter_bits=scb.CounterBits(bits))
+    b = scb.SuperCountingBloomBuilder(cfg)
+    for _ in range(3 if bits == 8 else 1):  # repeats push u8 counters to saturation
+        b.add_sequences(data, offsets)
+    idx = b.into_index()
+    requests = [workloads.random_sequences(60, 5_000, 30_000, seed=300 + i, genome=genome) for i in range(6)]
+    expected = [idx.estimate_batch(d, o) for d, o in requests]
+    if bits == 8:
+        assert any(int(eo.max()) == 255 for eo, _ in expected)
+    srv = scb.SuperCountingBloomServer(idx, max_batch_bytes=4 << 20, max_inflight=2)
+    tickets = [srv.submit(d, o) for d, o in requests]
+    _check_all([srv.wait(t)[:2] for t in tickets], expected)
+    srv.close()
