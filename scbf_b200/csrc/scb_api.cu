@@ -180,6 +180,23 @@ __global__ void k_rebase(uint64_t* off, uint64_t n, uint64_t base) {
     if (i < n) off[i] -= base;
 }
 
+// Narrows a batch's u64 estimates (out, cleared past the batch's windows) to `width` bytes each
+// for the copy to the host: the first n entries, or the batch's byte count (an upper bound of its
+// windows) from the parameter block on graph replays.
+__global__ void k_narrow_out(const BatchParams* __restrict__ bp, uint64_t n, const unsigned long long* __restrict__ out,
+                             void* __restrict__ outn, uint32_t width) {
+    if (bp) n = bp->n_bytes;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const unsigned long long v = __ldcs(out + i);
+        if (width == 2) {
+            static_cast<uint16_t*>(outn)[i] = (uint16_t)v;
+        } else {
+            static_cast<uint32_t*>(outn)[i] = (uint32_t)v;
+        }
+    }
+}
+
 // Derived arrays of a batch of n_bytes (codes, bitmaps, counters).  The input buffers (ascii,
 // offsets) are left alone: they may hold an uploaded batch.
 scb_status ensure_lane_work(scb_ctx* ctx, Lane& L, uint64_t n_bytes) {
@@ -1178,6 +1195,12 @@ scb_status for_each_chunk(scb_ctx* ctx, const uint8_t* seqs, const uint64_t* off
 
 }  // namespace
 
+void scb::launch_narrow_out(const BatchParams* bp, uint64_t n, const unsigned long long* out, void* outn, uint32_t width,
+                            int sm_count, cudaStream_t st) {
+    k_narrow_out<<<(unsigned)(sm_count * 4), 256, 0, st>>>(bp, n, out, outn, width);
+    note_launch();
+}
+
 // ---------------------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------------------
@@ -1398,23 +1421,64 @@ static scb_status abund_batch(scb_ctx* ctx, Lane& L, TileArgs& a, uint64_t n_seq
     return query_device_batch(ctx, L, kModeAbund, a, st);
 }
 
+// Widens n estimates of `width` (2 or 4) bytes into u64, on the host's threads when n is large.
+static void widen_estimates(uint64_t* dst, const uint8_t* src, uint64_t n, uint32_t width) {
+    auto run = [&](uint64_t lo, uint64_t hi) {
+        if (width == 2) {
+            const uint16_t* s16 = reinterpret_cast<const uint16_t*>(src);
+            for (uint64_t j = lo; j < hi; j++) dst[j] = s16[j];
+        } else {
+            const uint32_t* s32 = reinterpret_cast<const uint32_t*>(src);
+            for (uint64_t j = lo; j < hi; j++) dst[j] = s32[j];
+        }
+    };
+    const uint64_t parts = std::min<uint64_t>(std::max(1u, std::thread::hardware_concurrency()), n >> 19);
+    if (parts <= 1) {
+        run(0, n);
+        return;
+    }
+    std::vector<std::thread> th;
+    for (uint64_t t = 1; t < parts; t++) th.emplace_back(run, n * t / parts, n * (t + 1) / parts);
+    run(0, n / parts);
+    for (auto& x : th) x.join();
+}
+
+// The per-window estimates cross PCIe at the counters' width (2 bytes for 8- and 16-bit counters, 4
+// for 32-bit ones) into pinned staging, and are widened into the caller's u64 buffer on the host.
 scb_status scb_query_batch(scb_ctx* ctx, const uint8_t* seqs, const uint64_t* offsets, uint64_t n, uint64_t* ab,
                            uint8_t* valid) {
     SCB_TRY(need_frozen(ctx));
     CtxLock lk(ctx);
-    DevBuf d_out, d_valid;
+    const uint32_t width = ctx->g.bits <= 16 ? 2u : 4u;
     SCB_TRY(for_each_chunk(ctx, seqs, offsets, n, [&](Lane& L, TileArgs& a, const Chunk& ch) -> scb_status {
         const uint64_t nw = windows_of(offsets + ch.seq0, ch.seq1 - ch.seq0, ctx->cfg.k);
-        SCB_TRY(d_out.ensure(std::max<uint64_t>(nw, 1) * 8));
-        SCB_TRY(d_valid.ensure(std::max<uint64_t>(nw, 1)));
-        SCB_TRY(abund_batch(ctx, L, a, ch.seq1 - ch.seq0, L.stream, d_out.as<unsigned long long>(),
-                            d_valid.as<uint8_t>(), nw));
+        SCB_TRY(L.qout.ensure(std::max<uint64_t>(nw, 1) * 8));
+        SCB_TRY(L.qvalid.ensure(std::max<uint64_t>(nw, 1)));
+        SCB_TRY(L.qnarrow.ensure(std::max<uint64_t>(nw, 1) * width));
+        SCB_TRY(abund_batch(ctx, L, a, ch.seq1 - ch.seq0, L.stream, L.qout.as<unsigned long long>(),
+                            L.qvalid.as<uint8_t>(), nw));
         if (nw) {
-            SCB_CUDA(cudaMemcpyAsync(ab + ch.win0, d_out.p, nw * 8, cudaMemcpyDeviceToHost, L.stream));
-            SCB_CUDA(cudaMemcpyAsync(valid + ch.win0, d_valid.p, nw, cudaMemcpyDeviceToHost, L.stream));
+            const uint64_t need = nw * (width + 1);
+            if (need > ctx->q_stage_bytes) {
+                SCB_CUDA(cudaStreamSynchronize(L.stream));
+                if (ctx->q_stage) cudaFreeHost(ctx->q_stage);
+                ctx->q_stage = nullptr;
+                ctx->q_stage_bytes = 0;
+                SCB_CUDA(cudaMallocHost((void**)&ctx->q_stage, need));
+                ctx->q_stage_bytes = need;
+            }
+            launch_narrow_out(nullptr, nw, L.qout.as<unsigned long long>(), L.qnarrow.p, width, ctx->sm_count,
+                              L.stream);
+            SCB_CUDA(cudaMemcpyAsync(ctx->q_stage, L.qnarrow.p, nw * width, cudaMemcpyDeviceToHost, L.stream));
+            SCB_CUDA(cudaMemcpyAsync(ctx->q_stage + nw * width, L.qvalid.p, nw, cudaMemcpyDeviceToHost, L.stream));
         }
         unsigned long long c[kCntSlots];
-        return read_counters(ctx, L, L.stream, c);
+        SCB_TRY(read_counters(ctx, L, L.stream, c));  // waits for the copies
+        if (nw) {
+            widen_estimates(ab + ch.win0, ctx->q_stage, nw, width);
+            std::memcpy(valid + ch.win0, ctx->q_stage + nw * width, nw);
+        }
+        return SCB_OK;
     }));
     return SCB_OK;
 }

@@ -172,6 +172,9 @@ struct Lane {
     // rec_count[2])
     DevBuf ditems, ditem_base;
     DevBuf kept;  // the build apply's per-CTA probe words (kKeptSmers per CTA)
+    // a host per-window query's outputs: u64 estimates, validity bytes, and the estimates narrowed
+    // to the counters' width for the copy to the host
+    DevBuf qout, qvalid, qnarrow;
     bool want_probes = false;
     bool want_build = false;  // the grouped insert of this batch is a build apply
     bool want_spectrum = false;  // buckets sized for the spectrum apply
@@ -213,6 +216,11 @@ struct Tuning {
     uint64_t host_batch_bytes = kMaxBatchBytes - 64;  // sequence bytes per batch of a host call
 };
 
+// Narrows u64 per-window estimates to `width` (2 or 4) bytes each for a copy to the host: the
+// first n entries, or bp->n_bytes of them when bp is given (graph replays).
+void launch_narrow_out(const BatchParams* bp, uint64_t n, const unsigned long long* out, void* outn, uint32_t width,
+                       int sm_count, cudaStream_t st);
+
 // Packs n sequence bytes on the host into the device layout of kernel (a) (codes: 16 bases per
 // 32-bit word; valid: 32 bases per word; kPadWords zero words after each), on up to `threads`
 // threads (scb_hostpack.cpp).
@@ -250,6 +258,9 @@ struct scb_ctx {
     uint64_t stage_groups = 0;
     cudaEvent_t stage_free[2] = {nullptr, nullptr};
     uint64_t h2d_bytes = 0;  // bytes the host entry points copied to the device (scb_h2d_bytes)
+    // pinned staging of a host per-window query's narrowed estimates and validity bytes
+    uint8_t* q_stage = nullptr;
+    uint64_t q_stage_bytes = 0;
     bool timing = false;
     bool graphs = true;  // replay batches through graphs captured per shape class
     bool fused_build = true;  // a grouped build + stream query answers exclusive buckets in its insert
@@ -257,6 +268,8 @@ struct scb_ctx {
     std::mutex mu;
     ~scb_ctx() {
         if (copy_stream) cudaStreamSynchronize(copy_stream);
+        if (lane.stream) cudaStreamSynchronize(lane.stream);
+        if (q_stage) cudaFreeHost(q_stage);
         for (int i = 0; i < 2; i++) {
             if (stage_codes[i]) cudaFreeHost(stage_codes[i]);
             if (stage_valid[i]) cudaFreeHost(stage_valid[i]);

@@ -206,23 +206,6 @@ scb_status scb_server::clear_spectrum(cudaStream_t st) {
     return SCB_OK;
 }
 
-// Narrows a batch's u64 estimates (out, cleared past the batch's windows) to `width` bytes each
-// for the copy to the host: the first n entries, or the batch's byte count (an upper bound of its
-// windows) from the parameter block on graph replays.
-__global__ void k_narrow_out(const BatchParams* __restrict__ bp, uint64_t n, const unsigned long long* __restrict__ out,
-                             void* __restrict__ outn, uint32_t width) {
-    if (bp) n = bp->n_bytes;
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        const unsigned long long v = __ldcs(out + i);
-        if (width == 2) {
-            static_cast<uint16_t*>(outn)[i] = (uint16_t)v;
-        } else {
-            static_cast<uint32_t*>(outn)[i] = (uint32_t)v;
-        }
-    }
-}
-
 // The graph body of one slot batch: sizes from the slot's parameter block, fixed grids.
 scb_status scb_server::record(Slot& s, cudaStream_t st) {
     const BatchParams* bp = s.params.as<BatchParams>();
@@ -241,8 +224,7 @@ scb_status scb_server::record(Slot& s, cudaStream_t st) {
     } else {
         launch_tiles(kModeAbund, a, tile_grid(kModeAbund, ctx->g.bits, sms, a.n_tiles), st);
     }
-    k_narrow_out<<<(unsigned)(sms * 4), 256, 0, st>>>(bp, 0, s.out.as<unsigned long long>(), s.outn.p, out_width);
-    note_launch();
+    launch_narrow_out(bp, 0, s.out.as<unsigned long long>(), s.outn.p, out_width, sms, st);
     SCB_CUDA(cudaGetLastError());
     return SCB_OK;
 }
@@ -322,9 +304,8 @@ scb_status scb_server::launch(Slot& s) {
                 launch_tiles(kModeAbund, a, tile_grid(kModeAbund, c->g.bits, c->sm_count, a.n_tiles), st);
             }
             if (wins) {
-                k_narrow_out<<<(unsigned)(c->sm_count * 4), 256, 0, st>>>(nullptr, wins, s.out.as<unsigned long long>(),
-                                                                           s.outn.p, out_width);
-                note_launch();
+                launch_narrow_out(nullptr, wins, s.out.as<unsigned long long>(), s.outn.p, out_width, c->sm_count,
+                                  st);
             }
             SCB_CUDA(cudaGetLastError());
         }
