@@ -1811,11 +1811,19 @@ scb_status scb_spectrum_distinct(scb_ctx* ctx, const uint8_t* seqs, const uint64
     SCB_TRY(need_frozen(ctx));
     CtxLock lk(ctx);
     SCB_TRY(check_offsets(offsets, n));
-    const uint64_t W = windows_of(offsets, n, ctx->cfg.k);
-    DevBuf set, hist, ovf;
+    // the context's buffers (grown, never freed per call: a free would synchronise the device)
+    DevBuf& set = ctx->spec_set;
+    DevBuf& hist = ctx->spec_hist;
+    DevBuf& ovf = ctx->spec_ovf;
     const uint32_t dense = ctx->g.bits == 8 ? 256u : 65536u;
     SCB_TRY(hist.ensure((uint64_t)dense * 8));
-    const uint64_t ovf_cap = ctx->g.bits == 32 ? std::max<uint64_t>(W, 1) : 1;
+    // the batch's window count bounds the overflow list (32-bit counters) and the tile kernel's key set
+    uint64_t W = ~0ull;
+    auto windows = [&]() {
+        if (W == ~0ull) W = windows_of(offsets, n, ctx->cfg.k);
+        return W;
+    };
+    const uint64_t ovf_cap = ctx->g.bits == 32 ? std::max<uint64_t>(windows(), 1) : 1;
     SCB_TRY(ovf.ensure(ovf_cap * 8));
     // the chunks run on the lane's stream, behind these clears
     SCB_TRY(ensure_lane_work(ctx, ctx->lane, 0));
@@ -1839,7 +1847,7 @@ scb_status scb_spectrum_distinct(scb_ctx* ctx, const uint8_t* seqs, const uint64
     const uint64_t total = n ? offsets[n] - offsets[0] : 0;
     const bool grouped = plan.size() == 1 && grouped_supported(ctx) &&
                          resolve(ctx, ctx->query_strategy, total, false) == SCB_STRATEGY_GROUPED;
-    if (!grouped) SCB_TRY(make_set(W));
+    if (!grouped) SCB_TRY(make_set(windows()));
     SCB_TRY(for_each_chunk(ctx, seqs, offsets, n, [&](Lane& L, TileArgs& a, const Chunk&) -> scb_status {
         a.hist = hist.as<unsigned long long>();
         a.hist_dense = dense;

@@ -258,6 +258,8 @@ struct scb_ctx {
     uint64_t stage_groups = 0;
     cudaEvent_t stage_free[2] = {nullptr, nullptr};
     uint64_t h2d_bytes = 0;  // bytes the host entry points copied to the device (scb_h2d_bytes)
+    // the distinct-k-mer spectrum's key set, dense histogram and overflow list (grown as needed)
+    scb::DevBuf spec_set, spec_hist, spec_ovf;
     // pinned staging of a host per-window query's narrowed estimates and validity bytes
     uint8_t* q_stage = nullptr;
     uint64_t q_stage_bytes = 0;
