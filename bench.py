@@ -16,7 +16,8 @@ Arms:
              shards, bounded queue, all host threads) on a bounded sample of the same workload.
 
 N > 1 runs N independent replicas (one table and one read set per GPU); value = k-mers of all
-ranks / the slowest rank's time.  Rank 0 prints one JSON line.
+ranks / the slowest rank's time.  Rank 0 prints one JSON line.  The single-GPU characterisations
+(serving, mixed lengths, spectrum, configuration 1, CPU baseline) run at N = 1 only.
 """
 from __future__ import annotations
 
@@ -561,7 +562,7 @@ def run_ours(args, dist: Dist):
         check(L.scb_freeze(c1.h))
         spectrum["config1"] = run_spectrum(L, c1.h, d1, o1, st1, 24)
         c1.close()
-    config1 = run_config1(L, args)
+    config1 = run_config1(L, args) if dist.world == 1 else None
     serving = None
     if not args.no_serve:
         check(L.scb_set_strategy(h, 0, 0))
@@ -1055,6 +1056,10 @@ def main():
         run_profile_case(args)
         return
     dist = Dist(args.gpus)
+    if dist.world > 1:
+        # the single-GPU characterisations (serving, mixed lengths, spectrum, configuration 1) run at
+        # N = 1; with N replicas every rank times the step, its strategies and the end-to-end call
+        args.no_serve = args.no_mixed = args.no_spectrum = True
     try:
         if args.impl == "reference":
             run_reference(args, dist)
