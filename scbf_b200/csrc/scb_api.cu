@@ -1563,7 +1563,6 @@ static bool pieces_apply(const scb_ctx* ctx, uint64_t total) {
 static scb_status preload_first_piece(scb_ctx* ctx, const uint8_t* seqs, const uint64_t* offsets, uint64_t n,
                                       uint64_t& pre) {
     pre = 0;
-    if (ctx->host_pack) return SCB_OK;  // the pieces are packed on the host first
     if (!seqs || !n || offsets[n] < offsets[0] || !pieces_apply(ctx, offsets[n] - offsets[0])) return SCB_OK;
     const uint64_t first = (uint64_t)ramp_first(piece_bytes_for(ctx, offsets[n] - offsets[0]));
     if (!first || first >= offsets[n] - offsets[0]) return SCB_OK;
@@ -1615,9 +1614,9 @@ static scb_status build_stream_pieces(scb_ctx* ctx, const uint8_t* seqs, const u
     // overlaps the GPU's work on the pieces already launched.  The first piece's bytes are already
     // on their way when it fits the preloaded size (a longer first sequence reallocates the
     // buffer, after the copy, and copies the piece again).
-    // With host packing (the default) the host packs each piece into the device layout in a pinned
-    // staging area (all host threads) and copies 3 bits per base instead of the 8-bit letters; it
-    // packs piece p + 1 while the GPU works on piece p.
+    // With host packing (the default) the host packs each piece after the first into the device
+    // layout in a pinned staging area (all host threads) and copies 3 bits per base instead of the
+    // 8-bit letters; it packs piece p + 1 while the GPU works on piece p.
     const bool hp = ctx->host_pack;
     PrepackedReset reset_marks{ctx};
     if (hp) {
@@ -1631,7 +1630,9 @@ static scb_status build_stream_pieces(scb_ctx* ctx, const uint8_t* seqs, const u
         Lane& L = *ctx->piece_lanes[p];
         const uint64_t ns = c.seq1 - c.seq0, nb = c.byte1 - c.byte0;
         SCB_TRY(ensure_lane(ctx, L, nb, ns));
-        if (hp) {
+        // the first piece goes as letters when they are already on their way (copied while the
+        // offsets were validated, so the GPU starts without waiting for the host to pack it)
+        if (hp && !(p == 0 && pre && nb <= pre)) {
             // the piece's graph sizes the lane's work buffers for its byte class: grow them before
             // the copy, so that no later growth drops the copied codes
             SCB_TRY(ensure_lane_work(ctx, L, std::max(nb, std::min(class_bytes(nb), kMaxBatchBytes - 64))));
